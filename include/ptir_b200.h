@@ -1,0 +1,177 @@
+/*
+ * ptir_b200 — C ABI of the B200-native Gaussian-field path tracer.
+ *
+ * Drop-in boundary for the native half of PTIR's `threedgptir_tracer` extension. Each entry
+ * point replaces one method of the reference's pybind11 class `OptixTracer`
+ * (threedgptir_tracer/bindings.cpp:32-38, include/3dgptir/optixTracer.h:130-217):
+ *
+ *   ptir_create      <- OptixTracer::OptixTracer   (optixTracer.h:130-144, optixTracer.cpp:274-343)
+ *   ptir_destroy     <- OptixTracer::~OptixTracer  (optixTracer.h:146, optixTracer.cpp:345-371)
+ *   ptir_build_bvh   <- OptixTracer::buildBVH      (optixTracer.h:212-217, optixTracer.cpp:633-907)
+ *   ptir_trace       <- OptixTracer::trace         (optixTracer.h:148-168, optixTracer.cpp:909-1013)
+ *   ptir_trace_bwd   <- OptixTracer::traceBwd      (optixTracer.h:170-210, optixTracer.cpp:1015-1145)
+ *   ptir_last_error  <- (new) the reference logs CUDA/OptiX errors without raising
+ *                       (cuoptixMacros.h:22-44); here every entry returns a status and the
+ *                       message is kept on the handle.
+ *
+ * Conventions
+ *   - Every pointer named in an args struct is DEVICE memory, float32, C-contiguous, in the
+ *     reference's tensor layout; the caller owns all of it (inputs and outputs), as torch does
+ *     for the reference (optixTracer.cpp:931-944, 1057-1063). Output buffers need no
+ *     initialisation: every element is written (the reference's zero-filled outputs are
+ *     written as zeros).
+ *   - The library owns its acceleration structure and scratch; buffers grow, never shrink.
+ *   - All work is enqueued on `stream` (a cudaStream_t); no entry point synchronises the host
+ *     with the device, so a trace can be captured in a CUDA graph once the structure exists.
+ *   - Return value: PTIR_OK (0) or a PTIR_E* code; ptir_last_error() describes the last failure.
+ *   - A handle is not thread-safe (nor is the reference's object).
+ */
+#ifndef PTIR_B200_H
+#define PTIR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PTIR_ABI_VERSION 1
+
+enum {
+    PTIR_OK = 0,
+    PTIR_EINVAL = 1,   /* bad argument: shape, null pointer, unsupported option */
+    PTIR_ECUDA = 2,    /* a CUDA call failed */
+    PTIR_ESTATE = 3,   /* trace before build_bvh, or particle count differs from the structure */
+    PTIR_EDEVICE = 4,  /* a kernel hit one of its loop bounds (reported by ptir_device_status) */
+};
+
+typedef struct ptir_tracer ptir_tracer;
+
+/* Construction options: the arguments of OptixTracer(...) that change the traced result
+ * (optixTracer.h:130-144; the JIT defines of optixTracer.cpp:240-272). The pipeline and
+ * primitive names of the reference select its OptiX programs; only the configured
+ * `reference` pipeline with `instances` primitives exists here. */
+typedef struct ptir_config {
+    float kernel_degree;          /* render.particle_kernel_degree (default 4) */
+    float kernel_min_response;    /* render.particle_kernel_min_response (0.0113) */
+    int32_t density_clamping;     /* render.particle_kernel_density_clamping */
+    int32_t sph_degree;           /* render.particle_radiance_sph_degree: rows hold (d+1)^2*3 floats */
+    int32_t enable_normals;       /* render.enable_normals */
+    int32_t enable_hitcounts;     /* render.enable_hitcounts */
+    int32_t enable_mis;           /* render.enable_mis */
+    int32_t enable_metallic;      /* render.enable_metallic */
+    int32_t visualize_lights;     /* render.visualize_lights */
+    int32_t collect_counters;     /* keep per-launch segment/candidate counters (cheap) */
+} ptir_config;
+
+/* Inputs of one trace, shared by the forward and the backward
+ * (the arguments of OptixTracer::trace, optixTracer.h:148-168). */
+typedef struct ptir_trace_args {
+    uint32_t frame;                 /* frameNumber: seeds the per-path random streams */
+    const float* ray_to_world;      /* [B,4,4]; only the first matrix is applied (optixTracer.cpp:962) */
+    const float* ray_origin;        /* [Z,H,W,3] */
+    const float* ray_direction;     /* [Z,H,W,3] */
+    int32_t z, h, w;                /* launch extent: Z = spp * B */
+    const float* particle_density;  /* [N,12]: pos3 density1 rot4(wxyz) scale3 pad1 */
+    const float* particle_material; /* [N,5]: albedo3 roughness1 metallic1 */
+    const float* particle_radiance; /* [N,(sph_degree+1)^2*3] SH coefficients, coefficient-major */
+    const float* particle_shading_normal; /* [N,3] */
+    int32_t n;                      /* N; must equal the count of the last ptir_build_bvh */
+    const float* environment;       /* [EH,EW,4] or NULL; cube map when EH == 6*EW */
+    int32_t env_h, env_w;
+    const float* environment_alias; /* [3,AH,AW] prob/alias/pdf or NULL */
+    int32_t alias_h, alias_w;
+    /* punctual / area light tables (tracer.py:40-119 LightBuffers); counts must be 0 */
+    int32_t num_lights, num_light_entries, num_mesh_lights;
+    uint32_t sh_indirect;           /* RenderOpts: 0 = NONE, 1 = INDIRECT */
+    int32_t sph_eval_degree;        /* SH degree evaluated (<= sph_degree) */
+    float min_transmittance;        /* render.min_transmittance */
+    uint32_t max_bounces;           /* render.max_bounces */
+} ptir_trace_args;
+
+/* Forward outputs, [Z,H,W,C] (optixTracer.cpp:931-944). */
+typedef struct ptir_trace_outputs {
+    float* radiance;                   /* C=3 */
+    float* density;                    /* C=1 (opacity) */
+    float* hit_distance;               /* C=2 (integrated depth, last hit distance) */
+    float* hit_distance_second_moment; /* C=1 */
+    float* depth_distortion;           /* C=1 */
+    float* normal;                     /* C=3 */
+    float* shading_normal;             /* C=3 */
+    float* material;                   /* C=5 */
+    float* hits_count;                 /* C=1 */
+    float* pbr;                        /* C=3 */
+    float* light;                      /* C=3 */
+    float* pbr_components;             /* [Z,H,W,2,3] direct / indirect */
+    float* visibility;                 /* [N,1]: int32 1 stored in the float32 element per visible Gaussian;
+                                          cleared by the call */
+} ptir_trace_outputs;
+
+/* Backward inputs: the saved forward outputs and the gradients flowing into them
+ * (OptixTracer::traceBwd, optixTracer.h:170-210). Gradients may be NULL (treated as zero). */
+typedef struct ptir_bwd_args {
+    const float* pbr;             /* [Z,H,W,3] forward rayPbr */
+    const float* light;           /* [Z,H,W,3] forward rayLight */
+    const float* pbr_grad;        /* [Z,H,W,3] */
+    const float* light_grad;      /* [Z,H,W,3] */
+    const float* material_grad;   /* [Z,H,W,5] */
+} ptir_bwd_args;
+
+/* Backward outputs. The reference's backward fills only the material and environment
+ * gradients; its density / SH / shading-normal gradients are zero tensors
+ * (optixTracer.cpp:1057-1063) and are left to the caller here. Both buffers are cleared by
+ * the call. */
+typedef struct ptir_bwd_outputs {
+    float* particle_material_grad; /* [N,5] */
+    float* environment_grad;       /* [EH,EW,4] or NULL */
+} ptir_bwd_outputs;
+
+/* Device counters of the most recent trace / trace_bwd (collect_counters = 1). */
+typedef struct ptir_counters {
+    uint64_t segments;      /* rays traced through the field: primary, shadow and bounce rays */
+    uint64_t trace_calls;   /* k-buffer traversals */
+    uint64_t candidates;    /* candidates returned by the traversals */
+    uint64_t accepted;      /* hits composited */
+    uint64_t env_lookups;   /* bilinear environment lookups */
+    uint64_t replay;        /* backward re-traversals of a segment */
+} ptir_counters;
+
+int ptir_abi_version(void);
+
+/* OptixTracer(path, cuda_path, pipeline, backwardPipeline, primitive, ...) */
+int ptir_create(const ptir_config* config, ptir_tracer** out);
+void ptir_destroy(ptir_tracer* tracer);
+
+/* buildBVH(mogPos[N,3], mogRot[N,4], mogScl[N,3], mogDns[N,1], rebuild, allow_update):
+ * a refit keeps the tree topology when rebuild == 0, allow_update != 0 and N is unchanged,
+ * like the reference's OPTIX_BUILD_OPERATION_UPDATE; otherwise the tree is rebuilt. */
+int ptir_build_bvh(ptir_tracer* tracer, const float* pos, const float* rot, const float* scl, const float* dns,
+                   int32_t n, int32_t rebuild, int32_t allow_update, void* stream);
+
+/* trace(...) -> 13 outputs */
+int ptir_trace(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_trace_outputs* out, void* stream);
+
+/* trace_bwd(...) -> (densityGrad, materialGrad, radianceGrad, shadingNormalGrad, environmentGrad) */
+int ptir_trace_bwd(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_bwd_args* bwd,
+                   const ptir_bwd_outputs* out, void* stream);
+
+/* Counters of the last launch; synchronises `stream`. */
+int ptir_get_counters(ptir_tracer* tracer, ptir_counters* out, void* stream);
+
+/* Bounded-loop status word of the last launches (0 = clean); synchronises `stream` and clears it. */
+int ptir_device_status(ptir_tracer* tracer, uint32_t* status_word, void* stream);
+
+/* Scene AABB of the current structure as 6 floats (lo.xyz, hi.xyz); synchronises `stream`. */
+int ptir_scene_bounds(ptir_tracer* tracer, float* out6, void* stream);
+
+/* Copies of the acceleration structure for tests: nodes [max(N-1,1)*16] floats,
+ * leaves [N*16] floats (see ptir_b200/csrc/device_types.h for the record layouts); synchronises. */
+int ptir_debug_accel(ptir_tracer* tracer, float* nodes_host, float* leaves_host, void* stream);
+
+const char* ptir_last_error(const ptir_tracer* tracer);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PTIR_B200_H */

@@ -1,0 +1,139 @@
+"""ctypes binding of ``libptir_b200.so`` (the C ABI declared in include/ptir_b200.h).
+
+The library is the only compute path: if it cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+_LIB = None
+
+PTIR_OK = 0
+PTIR_EINVAL = 1
+PTIR_ECUDA = 2
+PTIR_ESTATE = 3
+PTIR_EDEVICE = 4
+
+_FP = C.c_void_p  # device pointers are passed as integers
+
+
+class PtirConfig(C.Structure):
+    _fields_ = [
+        ("kernel_degree", C.c_float),
+        ("kernel_min_response", C.c_float),
+        ("density_clamping", C.c_int32),
+        ("sph_degree", C.c_int32),
+        ("enable_normals", C.c_int32),
+        ("enable_hitcounts", C.c_int32),
+        ("enable_mis", C.c_int32),
+        ("enable_metallic", C.c_int32),
+        ("visualize_lights", C.c_int32),
+        ("collect_counters", C.c_int32),
+    ]
+
+
+class PtirTraceArgs(C.Structure):
+    _fields_ = [
+        ("frame", C.c_uint32),
+        ("ray_to_world", _FP),
+        ("ray_origin", _FP),
+        ("ray_direction", _FP),
+        ("z", C.c_int32), ("h", C.c_int32), ("w", C.c_int32),
+        ("particle_density", _FP),
+        ("particle_material", _FP),
+        ("particle_radiance", _FP),
+        ("particle_shading_normal", _FP),
+        ("n", C.c_int32),
+        ("environment", _FP),
+        ("env_h", C.c_int32), ("env_w", C.c_int32),
+        ("environment_alias", _FP),
+        ("alias_h", C.c_int32), ("alias_w", C.c_int32),
+        ("num_lights", C.c_int32), ("num_light_entries", C.c_int32), ("num_mesh_lights", C.c_int32),
+        ("sh_indirect", C.c_uint32),
+        ("sph_eval_degree", C.c_int32),
+        ("min_transmittance", C.c_float),
+        ("max_bounces", C.c_uint32),
+    ]
+
+
+class PtirTraceOutputs(C.Structure):
+    _fields_ = [(k, _FP) for k in (
+        "radiance", "density", "hit_distance", "hit_distance_second_moment", "depth_distortion", "normal",
+        "shading_normal", "material", "hits_count", "pbr", "light", "pbr_components", "visibility")]
+
+
+class PtirBwdArgs(C.Structure):
+    _fields_ = [(k, _FP) for k in ("pbr", "light", "pbr_grad", "light_grad", "material_grad")]
+
+
+class PtirBwdOutputs(C.Structure):
+    _fields_ = [("particle_material_grad", _FP), ("environment_grad", _FP)]
+
+
+class PtirCounters(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("segments", "trace_calls", "candidates", "accepted", "env_lookups", "replay")]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", "ptir_trace", "ptir_trace_bwd",
+           "ptir_get_counters", "ptir_device_status", "ptir_scene_bounds", "ptir_debug_accel", "ptir_last_error")
+
+
+def lib_path() -> str:
+    return _build.LIB_PATH
+
+
+def load(build_if_missing: bool = True):
+    """Load the shared library (building it first when it is missing or stale)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if build_if_missing and _build.needs_build():
+        _build.build()
+    path = lib_path()
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: run `python -m ptir_b200.build`")
+    L = C.CDLL(path)
+    P = C.POINTER
+    L.ptir_abi_version.restype = C.c_int
+    L.ptir_create.argtypes = [P(PtirConfig), P(C.c_void_p)]
+    L.ptir_create.restype = C.c_int
+    L.ptir_destroy.argtypes = [C.c_void_p]
+    L.ptir_destroy.restype = None
+    L.ptir_build_bvh.argtypes = [C.c_void_p, _FP, _FP, _FP, _FP, C.c_int32, C.c_int32, C.c_int32, C.c_void_p]
+    L.ptir_build_bvh.restype = C.c_int
+    L.ptir_trace.argtypes = [C.c_void_p, P(PtirTraceArgs), P(PtirTraceOutputs), C.c_void_p]
+    L.ptir_trace.restype = C.c_int
+    L.ptir_trace_bwd.argtypes = [C.c_void_p, P(PtirTraceArgs), P(PtirBwdArgs), P(PtirBwdOutputs), C.c_void_p]
+    L.ptir_trace_bwd.restype = C.c_int
+    L.ptir_get_counters.argtypes = [C.c_void_p, P(PtirCounters), C.c_void_p]
+    L.ptir_get_counters.restype = C.c_int
+    L.ptir_device_status.argtypes = [C.c_void_p, P(C.c_uint32), C.c_void_p]
+    L.ptir_device_status.restype = C.c_int
+    L.ptir_scene_bounds.argtypes = [C.c_void_p, P(C.c_float), C.c_void_p]
+    L.ptir_scene_bounds.restype = C.c_int
+    L.ptir_debug_accel.argtypes = [C.c_void_p, _FP, _FP, C.c_void_p]
+    L.ptir_debug_accel.restype = C.c_int
+    L.ptir_last_error.argtypes = [C.c_void_p]
+    L.ptir_last_error.restype = C.c_char_p
+    _LIB = L
+    return L
+
+
+class PtirError(RuntimeError):
+    """Raised when a C-ABI call returns a non-zero status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"ptir error {code}: {message}")
+        self.code = code
+
+
+def check(handle, rc: int, what: str) -> None:
+    if rc != PTIR_OK:
+        msg = load().ptir_last_error(handle).decode(errors="replace") if handle else ""
+        raise PtirError(rc, f"{what}: {msg}")

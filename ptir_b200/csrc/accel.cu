@@ -1,0 +1,350 @@
+// LBVH build and refit (Karras 2012, "Maximizing Parallelism in the Construction of BVHs,
+// Octrees, and k-d Trees"), specialised to the Gaussian instance boxes of the tracer.
+//
+//   1. prep      per Gaussian: kernel support scale, world->instance map, instance AABB
+//                (the instance transform of threedgptir_tracer/src/particlePrimitives.cu:543-610)
+//   2. bounds    scene AABB (two-pass reduction)
+//   3. morton    63-bit Morton key of the AABB centre within the scene bounds
+//   4. sort      key/id radix sort (CUB)
+//   5. gather    leaf records in key order
+//   6. hierarchy internal nodes from the sorted keys (ties broken by position)
+//   7. refit     bottom-up child boxes with arrival counters
+// A refit (rebuild == false, same n) redoes 1, 2, 5 and 7 in the stored leaf order.
+#include <cub/device/device_radix_sort.cuh>
+
+#include "accel.h"
+#include "vecmath.cuh"
+
+namespace ptir {
+
+namespace {
+
+constexpr int kReduceBlocks = 296;  // 2 x 148 SMs
+constexpr int kReduceThreads = 256;
+
+// kernel support radius in units of the particle scale (particlePrimitives.cu:27-51)
+__device__ float support_scale(float density, float min_response, int clamping, float degree) {
+    const float modulation = clamping ? density : 1.0f;
+    const float min_resp = fminf(min_response / modulation, 0.97f);
+    if (degree < 0.0f) {
+        const float k = fabsf(degree);
+        const float s = 1.0f / powf(3.0f, k);
+        return powf((1.0f / (logf(min_resp) - 1.0f) + 1.0f) / s, 1.0f / k);
+    }
+    if (degree == 0.0f) return ((1.0f - min_resp) / 3.0f) / -0.329630334487f;
+    const float a = -4.5f / powf(3.0f, degree);
+    return powf(logf(min_resp) / a, 1.0f / degree);
+}
+
+__global__ void k_prep(int n, const float* __restrict__ pos, const float* __restrict__ rot, const float* __restrict__ scl,
+                       const float* __restrict__ dns, AccelBuildOptions opt, float4* __restrict__ inst,
+                       float4* __restrict__ box) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const float4 q = make_float4(rot[4 * g], rot[4 * g + 1], rot[4 * g + 2], rot[4 * g + 3]);
+    const Mat3 R = quat_r(q);
+    const float ks = support_scale(dns[g], opt.min_response, opt.density_clamping, opt.kernel_degree);
+    const float3 k = make_float3(scl[3 * g], scl[3 * g + 1], scl[3 * g + 2]) * ks;
+    const float3 mu = make_float3(pos[3 * g], pos[3 * g + 1], pos[3 * g + 2]);
+    // world = R diag(k) obj + mu  =>  obj = diag(1/k) R^T (world - mu)
+    const float3 a0 = make_float3(R.r0.x, R.r1.x, R.r2.x) * (1.0f / k.x);
+    const float3 a1 = make_float3(R.r0.y, R.r1.y, R.r2.y) * (1.0f / k.y);
+    const float3 a2 = make_float3(R.r0.z, R.r1.z, R.r2.z) * (1.0f / k.z);
+    const float kmax = fmaxf(k.x, fmaxf(k.y, k.z));
+    float4* rec = inst + 4 * (size_t)g;
+    rec[0] = make_float4(a0.x, a0.y, a0.z, -dot(a0, mu));
+    rec[1] = make_float4(a1.x, a1.y, a1.z, -dot(a1, mu));
+    rec[2] = make_float4(a2.x, a2.y, a2.z, -dot(a2, mu));
+    rec[3] = make_float4(__uint_as_float((unsigned)g), kmax, 0.0f, 0.0f);
+    // AABB of the 8 transformed corners of [-1,1]^3
+    float3 lo = f3(3.0e38f), hi = f3(-3.0e38f);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float3 corner = make_float3((c & 4) ? 1.0f : -1.0f, (c & 2) ? 1.0f : -1.0f, (c & 1) ? 1.0f : -1.0f);
+        const float3 v = mul_rows(R, corner * k) + mu;
+        lo = fmin3(lo, v);
+        hi = fmax3(hi, v);
+    }
+    box[2 * (size_t)g] = make_float4(lo.x, lo.y, lo.z, kmax);
+    box[2 * (size_t)g + 1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+}
+
+__device__ void block_minmax(float3& lo, float3& hi) {
+    __shared__ float3 slo[kReduceThreads / 32], shi[kReduceThreads / 32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        lo.x = fminf(lo.x, __shfl_xor_sync(0xFFFFFFFFu, lo.x, off));
+        lo.y = fminf(lo.y, __shfl_xor_sync(0xFFFFFFFFu, lo.y, off));
+        lo.z = fminf(lo.z, __shfl_xor_sync(0xFFFFFFFFu, lo.z, off));
+        hi.x = fmaxf(hi.x, __shfl_xor_sync(0xFFFFFFFFu, hi.x, off));
+        hi.y = fmaxf(hi.y, __shfl_xor_sync(0xFFFFFFFFu, hi.y, off));
+        hi.z = fmaxf(hi.z, __shfl_xor_sync(0xFFFFFFFFu, hi.z, off));
+    }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        slo[w] = lo;
+        shi[w] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < kReduceThreads / 32; ++i) {
+            lo = fmin3(lo, slo[i]);
+            hi = fmax3(hi, shi[i]);
+        }
+    }
+}
+
+__global__ void k_bounds_partial(int n, const float4* __restrict__ box, float4* __restrict__ partial) {
+    float3 lo = f3(3.0e38f), hi = f3(-3.0e38f);
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n; g += gridDim.x * blockDim.x) {
+        const float4 a = box[2 * (size_t)g], b = box[2 * (size_t)g + 1];
+        lo = fmin3(lo, make_float3(a.x, a.y, a.z));
+        hi = fmax3(hi, make_float3(b.x, b.y, b.z));
+    }
+    block_minmax(lo, hi);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+        partial[2 * blockIdx.x + 1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+    }
+}
+
+__global__ void k_bounds_final(int parts, const float4* __restrict__ partial, float4* __restrict__ bounds) {
+    float3 lo = f3(3.0e38f), hi = f3(-3.0e38f);
+    for (int i = threadIdx.x; i < parts; i += blockDim.x) {
+        const float4 a = partial[2 * i], b = partial[2 * i + 1];
+        lo = fmin3(lo, make_float3(a.x, a.y, a.z));
+        hi = fmax3(hi, make_float3(b.x, b.y, b.z));
+    }
+    block_minmax(lo, hi);
+    if (threadIdx.x == 0) {
+        bounds[0] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+        bounds[1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+    }
+}
+
+// spread the low 21 bits of v to every third bit
+__device__ unsigned long long spread3(unsigned long long v) {
+    v &= 0x1FFFFFull;
+    v = (v | (v << 32)) & 0x001F00000000FFFFull;
+    v = (v | (v << 16)) & 0x001F0000FF0000FFull;
+    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void k_morton(int n, const float4* __restrict__ box, const float4* __restrict__ bounds,
+                         unsigned long long* __restrict__ keys, unsigned* __restrict__ ids) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n) return;
+    const float4 a = box[2 * (size_t)g], b = box[2 * (size_t)g + 1];
+    const float4 lo = bounds[0], hi = bounds[1];
+    const float3 c = make_float3(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z));
+    const float3 ext = make_float3(fmaxf(hi.x - lo.x, 1e-30f), fmaxf(hi.y - lo.y, 1e-30f), fmaxf(hi.z - lo.z, 1e-30f));
+    const float scale = 2097151.0f;  // 2^21 - 1
+    const unsigned long long qx = (unsigned long long)fminf(fmaxf((c.x - lo.x) / ext.x, 0.0f) * scale, scale);
+    const unsigned long long qy = (unsigned long long)fminf(fmaxf((c.y - lo.y) / ext.y, 0.0f) * scale, scale);
+    const unsigned long long qz = (unsigned long long)fminf(fmaxf((c.z - lo.z) / ext.z, 0.0f) * scale, scale);
+    keys[g] = (spread3(qx) << 2) | (spread3(qy) << 1) | spread3(qz);
+    ids[g] = (unsigned)g;
+}
+
+__global__ void k_gather(int n, const unsigned* __restrict__ order, const float4* __restrict__ inst, float4* __restrict__ leaves) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const unsigned g = order[i];
+    const float4* src = inst + 4 * (size_t)g;
+    float4* dst = leaves + 4 * (size_t)i;
+    dst[0] = src[0];
+    dst[1] = src[1];
+    dst[2] = src[2];
+    dst[3] = src[3];
+}
+
+// common-prefix length of sorted keys i and j; equal keys fall back to the positions
+__device__ __forceinline__ int prefix(const unsigned long long* __restrict__ keys, int n, int i, int j) {
+    if (j < 0 || j >= n) return -1;
+    const unsigned long long a = keys[i], b = keys[j];
+    if (a == b) return 64 + __clz((unsigned)(i ^ j));
+    return __clzll(a ^ b);
+}
+
+__global__ void k_hierarchy(int n, const unsigned long long* __restrict__ keys, float4* __restrict__ nodes, int* __restrict__ parent) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    const int dir = (prefix(keys, n, i, i + 1) - prefix(keys, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = prefix(keys, n, i, i - dir);
+    int lmax = 2;
+    while (prefix(keys, n, i, i + lmax * dir) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (prefix(keys, n, i, i + (l + t) * dir) > dmin) l += t;
+    const int j = i + l * dir;
+    const int dnode = prefix(keys, n, i, j);
+    int s = 0;
+    for (int div = 2;; div <<= 1) {
+        const int t = (l + div - 1) / div;
+        if (prefix(keys, n, i, i + (s + t) * dir) > dnode) s += t;
+        if (t <= 1) break;
+    }
+    const int split = i + s * dir + min(dir, 0);
+    const int lo = min(i, j), hi = max(i, j);
+    const int left = (lo == split) ? ~split : split;
+    const int right = (hi == split + 1) ? ~(split + 1) : split + 1;
+    nodes[4 * (size_t)i + 3] = make_float4(__int_as_float(left), __int_as_float(right), 0.0f, 0.0f);
+    parent[left < 0 ? (n - 1) + ~left : left] = i;
+    parent[right < 0 ? (n - 1) + ~right : right] = i;
+    if (i == 0) parent[0] = -1;
+}
+
+// box and kmax of child c of the hierarchy
+__device__ __forceinline__ void child_box(const float4* __restrict__ sbox_unsorted, const unsigned* __restrict__ order,
+                                          const float4* nodes, int c, float3& lo, float3& hi, float& kmax) {
+    if (c < 0) {
+        const unsigned g = order[~c];
+        const float4 a = sbox_unsorted[2 * (size_t)g], b = sbox_unsorted[2 * (size_t)g + 1];
+        lo = make_float3(a.x, a.y, a.z);
+        hi = make_float3(b.x, b.y, b.z);
+        kmax = a.w;
+        return;
+    }
+    const float4* nd = nodes + 4 * (size_t)c;
+    const float4 a = __ldcg(nd), b = __ldcg(nd + 1), e = __ldcg(nd + 2), f = __ldcg(nd + 3);
+    lo = fmin3(make_float3(a.x, a.y, a.z), make_float3(b.z, b.w, e.x));
+    hi = fmax3(make_float3(a.w, b.x, b.y), make_float3(e.y, e.z, e.w));
+    kmax = fmaxf(f.z, f.w);
+}
+
+__global__ void k_refit(int n, const float4* __restrict__ box, const unsigned* __restrict__ order, float4* nodes,
+                        const int* __restrict__ parent, unsigned* arrivals) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int p = parent[(n - 1) + j];
+    while (p >= 0) {
+        __threadfence();
+        if (atomicAdd(arrivals + p, 1u) == 0u) return;  // the sibling subtree is not finished yet
+        __threadfence();
+        float4* nd = nodes + 4 * (size_t)p;
+        const float4 f = __ldcg(nd + 3);
+        const int left = __float_as_int(f.x), right = __float_as_int(f.y);
+        float3 llo, lhi, rlo, rhi;
+        float lk, rk;
+        child_box(box, order, nodes, left, llo, lhi, lk);
+        child_box(box, order, nodes, right, rlo, rhi, rk);
+        __stcg(nd + 0, make_float4(llo.x, llo.y, llo.z, lhi.x));
+        __stcg(nd + 1, make_float4(lhi.y, lhi.z, rlo.x, rlo.y));
+        __stcg(nd + 2, make_float4(rlo.z, rhi.x, rhi.y, rhi.z));
+        __stcg(nd + 3, make_float4(f.x, f.y, lk, rk));
+        p = parent[p];
+    }
+}
+
+template <class T>
+cudaError_t grow(T*& ptr, size_t count, cudaStream_t s) {
+    if (ptr) {
+        cudaError_t e = cudaFreeAsync(ptr, s);
+        if (e != cudaSuccess) return e;
+        ptr = nullptr;
+    }
+    return cudaMallocAsync(reinterpret_cast<void**>(&ptr), count * sizeof(T), s);
+}
+
+}  // namespace
+
+cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const float* pos, const float* rot,
+                        const float* scl, const float* dns, int n, bool rebuild, cudaStream_t s, std::string& err) {
+    cudaError_t e = cudaSuccess;
+#define PTIR_TRY(expr)                                     \
+    do {                                                   \
+        e = (expr);                                        \
+        if (e != cudaSuccess) {                            \
+            err = std::string(#expr) + ": " + cudaGetErrorString(e); \
+            st.valid = false;                              \
+            return e;                                      \
+        }                                                  \
+    } while (0)
+    if (n < 0) {
+        err = "negative Gaussian count";
+        return cudaErrorInvalidValue;
+    }
+    const bool refit = !rebuild && st.valid && st.n == n && n > 1;
+    if (!st.bounds) PTIR_TRY(cudaMallocAsync(reinterpret_cast<void**>(&st.bounds), 2 * sizeof(float4), s));
+    if (!st.partial) PTIR_TRY(cudaMallocAsync(reinterpret_cast<void**>(&st.partial), 2 * kReduceBlocks * sizeof(float4), s));
+    st.n = n;
+    if (n == 0) {
+        st.valid = true;
+        return cudaSuccess;
+    }
+    if ((size_t)n > st.capacity) {
+        const size_t cap = (size_t)n;
+        PTIR_TRY(grow(st.inst, 4 * cap, s));
+        PTIR_TRY(grow(st.box, 2 * cap, s));
+        PTIR_TRY(grow(st.keys[0], cap, s));
+        PTIR_TRY(grow(st.keys[1], cap, s));
+        PTIR_TRY(grow(st.ids[0], cap, s));
+        PTIR_TRY(grow(st.ids[1], cap, s));
+        PTIR_TRY(grow(st.leaves, 4 * cap, s));
+        PTIR_TRY(grow(st.nodes, 4 * (cap > 1 ? cap - 1 : 1), s));
+        PTIR_TRY(grow(st.parent, 2 * cap, s));
+        PTIR_TRY(grow(st.arrivals, cap, s));
+        st.capacity = cap;
+        st.valid = false;
+    }
+    const int T = 256;
+    const unsigned blocks = (unsigned)((n + T - 1) / T);
+    k_prep<<<blocks, T, 0, s>>>(n, pos, rot, scl, dns, opt, st.inst, st.box);
+    PTIR_TRY(cudaGetLastError());
+    k_bounds_partial<<<kReduceBlocks, kReduceThreads, 0, s>>>(n, st.box, st.partial);
+    k_bounds_final<<<1, kReduceThreads, 0, s>>>(kReduceBlocks, st.partial, st.bounds);
+    PTIR_TRY(cudaGetLastError());
+    if (!refit) {
+        k_morton<<<blocks, T, 0, s>>>(n, st.box, st.bounds, st.keys[0], st.ids[0]);
+        PTIR_TRY(cudaGetLastError());
+        size_t need = 0;
+        PTIR_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, 63, s));
+        if (need > st.sort_temp_bytes) {
+            if (st.sort_temp) PTIR_TRY(cudaFreeAsync(st.sort_temp, s));
+            st.sort_temp = nullptr;
+            PTIR_TRY(cudaMallocAsync(&st.sort_temp, need, s));
+            st.sort_temp_bytes = need;
+        }
+        size_t have = st.sort_temp_bytes;
+        PTIR_TRY(cub::DeviceRadixSort::SortPairs(st.sort_temp, have, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, 63, s));
+        if (n > 1) {
+            k_hierarchy<<<(unsigned)((n - 1 + T - 1) / T), T, 0, s>>>(n, st.keys[1], st.nodes, st.parent);
+            PTIR_TRY(cudaGetLastError());
+        }
+    }
+    k_gather<<<blocks, T, 0, s>>>(n, st.ids[1], st.inst, st.leaves);
+    PTIR_TRY(cudaGetLastError());
+    if (n > 1) {
+        PTIR_TRY(cudaMemsetAsync(st.arrivals, 0, sizeof(unsigned) * (size_t)(n - 1), s));
+        k_refit<<<blocks, T, 0, s>>>(n, st.box, st.ids[1], st.nodes, st.parent, st.arrivals);
+        PTIR_TRY(cudaGetLastError());
+    }
+    st.valid = true;
+    return cudaSuccess;
+#undef PTIR_TRY
+}
+
+void accel_free(AccelState& st) {
+    auto rel = [](void* p) {
+        if (p) cudaFree(p);
+    };
+    rel(st.inst);
+    rel(st.box);
+    rel(st.keys[0]);
+    rel(st.keys[1]);
+    rel(st.ids[0]);
+    rel(st.ids[1]);
+    rel(st.leaves);
+    rel(st.nodes);
+    rel(st.parent);
+    rel(st.arrivals);
+    rel(st.partial);
+    rel(st.bounds);
+    rel(st.sort_temp);
+    st = AccelState();
+}
+
+}  // namespace ptir

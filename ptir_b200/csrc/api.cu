@@ -1,0 +1,299 @@
+// C ABI of the tracer (include/ptir_b200.h): argument checks, state, launches.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/ptir_b200.h"
+#include "accel.h"
+#include "device_types.h"
+
+struct ptir_tracer {
+    ptir_config cfg;
+    ptir::AccelState accel;
+    unsigned* error_word = nullptr;
+    unsigned long long* counters = nullptr;
+    std::string last_error;
+};
+
+namespace {
+
+int fail(ptir_tracer* t, int code, const std::string& msg) {
+    if (t) t->last_error = msg;
+    return code;
+}
+
+int cuda_fail(ptir_tracer* t, cudaError_t e, const char* what) {
+    return fail(t, PTIR_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+unsigned flags_of(const ptir_config& c) {
+    unsigned f = 0;
+    if (c.enable_normals) f |= ptir::kNormals;
+    if (c.enable_hitcounts) f |= ptir::kHitCounts;
+    if (c.enable_mis) f |= ptir::kMis;
+    if (c.enable_metallic) f |= ptir::kMetallic;
+    if (c.visualize_lights) f |= ptir::kVisualizeLights;
+    return f;
+}
+
+// checks shared by trace and trace_bwd; fills the kernel parameters
+int prepare(ptir_tracer* t, const ptir_trace_args* a, ptir::TraceParams& p) {
+    if (!a) return fail(t, PTIR_EINVAL, "null trace arguments");
+    if (a->z < 0 || a->h < 0 || a->w < 0) return fail(t, PTIR_EINVAL, "negative launch extent");
+    const long long launches = (long long)a->z * a->h * a->w;
+    if (launches > 0 && (!a->ray_origin || !a->ray_direction || !a->ray_to_world))
+        return fail(t, PTIR_EINVAL, "ray_origin, ray_direction and ray_to_world are required");
+    if (launches > (1ll << 31) - 1) return fail(t, PTIR_EINVAL, "launch extent exceeds 2^31 - 1 paths");
+    if (!t->accel.valid) return fail(t, PTIR_ESTATE, "trace called before build_bvh");
+    if (a->n != t->accel.n)
+        return fail(t, PTIR_ESTATE, "particle count " + std::to_string(a->n) + " differs from the acceleration structure (" +
+                                        std::to_string(t->accel.n) + ")");
+    if (a->n > 0 && (!a->particle_density || !a->particle_material || !a->particle_radiance))
+        return fail(t, PTIR_EINVAL, "particle density, material and radiance are required");
+    if (t->cfg.enable_normals && a->n > 0 && !a->particle_shading_normal)
+        return fail(t, PTIR_EINVAL, "particle_shading_normal is required when normals are enabled");
+    if (a->sph_eval_degree < 0 || a->sph_eval_degree > t->cfg.sph_degree || a->sph_eval_degree > 3)
+        return fail(t, PTIR_EINVAL, "sph_eval_degree must lie in [0, min(3, sph_degree)]");
+    if (a->num_lights != 0 || a->num_light_entries != 0 || a->num_mesh_lights != 0)
+        return fail(t, PTIR_EINVAL, "point, sphere and mesh lights are not supported (environment lighting only)");
+    if ((reinterpret_cast<uintptr_t>(a->particle_density) & 15u) != 0)
+        return fail(t, PTIR_EINVAL, "particle_density must be 16-byte aligned");
+    const bool env = a->environment != nullptr && a->env_h > 0 && a->env_w > 0;
+    if (env && (reinterpret_cast<uintptr_t>(a->environment) & 15u) != 0)
+        return fail(t, PTIR_EINVAL, "environment must be 16-byte aligned");
+    const bool alias = a->environment_alias != nullptr && a->alias_h > 0 && a->alias_w > 0;
+
+    std::memset(&p, 0, sizeof(p));
+    p.accel = t->accel.view();
+    p.part.density = reinterpret_cast<const float4*>(a->particle_density);
+    p.part.material = a->particle_material;
+    p.part.sph = a->particle_radiance;
+    p.part.snrm = a->particle_shading_normal;
+    p.part.sph_stride = (t->cfg.sph_degree + 1) * (t->cfg.sph_degree + 1) * 3;
+    p.part.sph_degree = a->sph_eval_degree;
+    p.env.data = env ? reinterpret_cast<const float4*>(a->environment) : nullptr;
+    p.env.w = env ? a->env_w : 0;
+    p.env.h = env ? a->env_h : 0;
+    p.env.cube = env && a->env_h == 6 * a->env_w;
+    if (alias) {
+        p.env.aw = a->alias_w;
+        p.env.ah = a->alias_h;
+        p.env.cells = a->alias_w * a->alias_h;
+        p.env.prob = a->environment_alias;
+        p.env.alias = a->environment_alias + p.env.cells;
+        p.env.pdf = a->environment_alias + 2 * p.env.cells;
+    }
+    // environment offset is fixed at (0, 0): rotation about z by pi/2, none about x
+    const float rot_z = 0.5f * 3.14159265358979323846f;
+    p.env.sin_z = (float)std::sin((double)rot_z);
+    p.env.cos_z = (float)std::cos((double)rot_z);
+    p.env.sin_x = 0.0f;
+    p.env.cos_x = 1.0f;
+    p.ray_to_world = a->ray_to_world;
+    p.ray_ori = a->ray_origin;
+    p.ray_dir = a->ray_direction;
+    p.nz = a->z;
+    p.h = a->h;
+    p.w = a->w;
+    p.frame = a->frame;
+    p.flags = flags_of(t->cfg);
+    p.kernel_degree = (int)t->cfg.kernel_degree;
+    p.min_response = t->cfg.kernel_min_response;
+    p.alpha_min = 1.0f / 255.0f;
+    p.min_transmittance = a->min_transmittance;
+    p.max_bounces = a->max_bounces;
+    p.render_opts = a->sh_indirect ? 1u : 0u;
+    p.error_word = t->error_word;
+    p.counters = t->cfg.collect_counters ? t->counters : nullptr;
+    return PTIR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptir_abi_version(void) { return PTIR_ABI_VERSION; }
+
+int ptir_create(const ptir_config* config, ptir_tracer** out) {
+    if (!config || !out) return PTIR_EINVAL;
+    *out = nullptr;
+    if (config->sph_degree < 0 || config->sph_degree > 3) return PTIR_EINVAL;
+    const float deg = config->kernel_degree;
+    const int ideg = (int)deg;
+    if (!(ideg == 0 || ideg == 1 || ideg == 2 || ideg == 3 || ideg == 4 || ideg == 5 || ideg == 8)) return PTIR_EINVAL;
+    if (!(config->kernel_min_response > 0.0f && config->kernel_min_response < 1.0f)) return PTIR_EINVAL;
+    ptir_tracer* t = new ptir_tracer();
+    t->cfg = *config;
+    if (cudaMalloc(&t->error_word, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&t->counters, sizeof(unsigned long long) * ptir::kNumCounters) != cudaSuccess) {
+        cudaFree(t->error_word);
+        cudaFree(t->counters);
+        delete t;
+        return PTIR_ECUDA;
+    }
+    cudaMemset(t->error_word, 0, sizeof(unsigned));
+    cudaMemset(t->counters, 0, sizeof(unsigned long long) * ptir::kNumCounters);
+    *out = t;
+    return PTIR_OK;
+}
+
+void ptir_destroy(ptir_tracer* t) {
+    if (!t) return;
+    cudaDeviceSynchronize();
+    ptir::accel_free(t->accel);
+    cudaFree(t->error_word);
+    cudaFree(t->counters);
+    delete t;
+}
+
+int ptir_build_bvh(ptir_tracer* t, const float* pos, const float* rot, const float* scl, const float* dns, int32_t n,
+                   int32_t rebuild, int32_t allow_update, void* stream) {
+    if (!t) return PTIR_EINVAL;
+    if (n < 0) return fail(t, PTIR_EINVAL, "negative particle count");
+    if (n > 0 && (!pos || !rot || !scl || !dns)) return fail(t, PTIR_EINVAL, "null particle pointer");
+    ptir::AccelBuildOptions opt{t->cfg.kernel_degree, t->cfg.kernel_min_response, t->cfg.density_clamping};
+    // the reference refits only when asked and allowed and the count is unchanged (optixTracer.cpp:646-649, 819-822)
+    const bool do_rebuild = rebuild != 0 || allow_update == 0 || n != t->accel.n;
+    std::string err;
+    const cudaError_t e = ptir::accel_build(t->accel, opt, pos, rot, scl, dns, n, do_rebuild, as_stream(stream), err);
+    if (e != cudaSuccess) return fail(t, PTIR_ECUDA, "build_bvh: " + err);
+    return PTIR_OK;
+}
+
+int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_outputs* o, void* stream) {
+    if (!t) return PTIR_EINVAL;
+    ptir::TraceParams p;
+    const int rc = prepare(t, a, p);
+    if (rc != PTIR_OK) return rc;
+    if (!o) return fail(t, PTIR_EINVAL, "null outputs");
+    const long long launches = (long long)a->z * a->h * a->w;
+    if (launches > 0 && (!o->radiance || !o->density || !o->hit_distance || !o->hit_distance_second_moment ||
+                         !o->depth_distortion || !o->normal || !o->shading_normal || !o->material || !o->hits_count ||
+                         !o->pbr || !o->light || !o->pbr_components))
+        return fail(t, PTIR_EINVAL, "every per-sample output buffer is required");
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e;
+    if (o->visibility && a->n > 0) {
+        e = cudaMemsetAsync(o->visibility, 0, sizeof(float) * (size_t)a->n, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "clear visibility");
+    }
+    if (p.counters) {
+        e = cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long) * ptir::kNumCounters, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "clear counters");
+    }
+    ptir::FwdOutputs fo;
+    fo.radiance = o->radiance;
+    fo.density = o->density;
+    fo.hit = o->hit_distance;
+    fo.hit2 = o->hit_distance_second_moment;
+    fo.distortion = o->depth_distortion;
+    fo.normal = o->normal;
+    fo.snormal = o->shading_normal;
+    fo.material = o->material;
+    fo.hits_count = o->hits_count;
+    fo.pbr = o->pbr;
+    fo.light = o->light;
+    fo.components = o->pbr_components;
+    fo.visibility = o->visibility;
+    e = ptir::launch_trace_fwd(p, fo, 128, s);
+    if (e != cudaSuccess) return cuda_fail(t, e, "trace launch");
+    return PTIR_OK;
+}
+
+int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args* b, const ptir_bwd_outputs* o,
+                   void* stream) {
+    if (!t) return PTIR_EINVAL;
+    ptir::TraceParams p;
+    const int rc = prepare(t, a, p);
+    if (rc != PTIR_OK) return rc;
+    if (!b || !o) return fail(t, PTIR_EINVAL, "null backward arguments");
+    const long long launches = (long long)a->z * a->h * a->w;
+    if (launches > 0 && (!b->pbr || !b->light)) return fail(t, PTIR_EINVAL, "forward pbr and light are required");
+    if (a->n > 0 && !o->particle_material_grad) return fail(t, PTIR_EINVAL, "particle_material_grad is required");
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e;
+    if (a->n > 0) {
+        e = cudaMemsetAsync(o->particle_material_grad, 0, sizeof(float) * 5 * (size_t)a->n, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "clear material grad");
+    }
+    const bool env = p.env.data != nullptr;
+    if (env && o->environment_grad) {
+        e = cudaMemsetAsync(o->environment_grad, 0, sizeof(float) * 4 * (size_t)p.env.w * p.env.h, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "clear environment grad");
+    }
+    if (p.counters) {
+        e = cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long) * ptir::kNumCounters, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "clear counters");
+    }
+    ptir::BwdInputs bi;
+    bi.pbr = b->pbr;
+    bi.light = b->light;
+    bi.pbr_grad = b->pbr_grad;
+    bi.light_grad = b->light_grad;
+    bi.material_grad = b->material_grad;
+    bi.particle_material_grad = o->particle_material_grad;
+    bi.environment_grad = env ? o->environment_grad : nullptr;
+    e = ptir::launch_trace_bwd(p, bi, 128, s);
+    if (e != cudaSuccess) return cuda_fail(t, e, "trace_bwd launch");
+    return PTIR_OK;
+}
+
+int ptir_get_counters(ptir_tracer* t, ptir_counters* out, void* stream) {
+    if (!t || !out) return PTIR_EINVAL;
+    unsigned long long h[ptir::kNumCounters];
+    cudaError_t e = cudaMemcpyAsync(h, t->counters, sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    if (e != cudaSuccess) return cuda_fail(t, e, "read counters");
+    out->segments = h[ptir::kCtrSegments];
+    out->trace_calls = h[ptir::kCtrTraceCalls];
+    out->candidates = h[ptir::kCtrCandidates];
+    out->accepted = h[ptir::kCtrAccepted];
+    out->env_lookups = h[ptir::kCtrEnvLookups];
+    out->replay = h[ptir::kCtrReplay];
+    return PTIR_OK;
+}
+
+int ptir_device_status(ptir_tracer* t, uint32_t* status_word, void* stream) {
+    if (!t || !status_word) return PTIR_EINVAL;
+    unsigned h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, t->error_word, sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess) e = cudaMemsetAsync(t->error_word, 0, sizeof(unsigned), as_stream(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    if (e != cudaSuccess) return cuda_fail(t, e, "read device status");
+    *status_word = h;
+    return h ? fail(t, PTIR_EDEVICE, "a kernel exceeded a loop bound (status " + std::to_string(h) + ")") : PTIR_OK;
+}
+
+int ptir_scene_bounds(ptir_tracer* t, float* out6, void* stream) {
+    if (!t || !out6) return PTIR_EINVAL;
+    if (!t->accel.valid || t->accel.n == 0) return fail(t, PTIR_ESTATE, "no acceleration structure");
+    float4 h[2];
+    cudaError_t e = cudaMemcpyAsync(h, t->accel.bounds, sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    if (e != cudaSuccess) return cuda_fail(t, e, "read bounds");
+    out6[0] = h[0].x; out6[1] = h[0].y; out6[2] = h[0].z;
+    out6[3] = h[1].x; out6[4] = h[1].y; out6[5] = h[1].z;
+    return PTIR_OK;
+}
+
+int ptir_debug_accel(ptir_tracer* t, float* nodes_host, float* leaves_host, void* stream) {
+    if (!t) return PTIR_EINVAL;
+    if (!t->accel.valid) return fail(t, PTIR_ESTATE, "no acceleration structure");
+    const int n = t->accel.n;
+    cudaStream_t s = as_stream(stream);
+    cudaError_t e = cudaSuccess;
+    if (nodes_host && n > 1)
+        e = cudaMemcpyAsync(nodes_host, t->accel.nodes, sizeof(float4) * 4 * (size_t)(n - 1), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && leaves_host && n > 0)
+        e = cudaMemcpyAsync(leaves_host, t->accel.leaves, sizeof(float4) * 4 * (size_t)n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(t, e, "copy acceleration structure");
+    return PTIR_OK;
+}
+
+const char* ptir_last_error(const ptir_tracer* t) { return t ? t->last_error.c_str() : "null tracer"; }
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// Plain-old-data views handed from the C-ABI layer to the kernels (by value, as kernel
+// parameters). Every pointer is device memory.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ptir {
+
+// Acceleration structure over the Gaussians' instance boxes: a binary LBVH whose internal
+// node i stores the AABBs of both children (so one 64-byte fetch tests two boxes) and whose
+// leaves are the Morton-ordered instance records.
+//   node  = 4 x float4: (L.lo.xyz, L.hi.x) (L.hi.yz, R.lo.xy) (R.lo.z, R.hi.xyz)
+//           (left, right, kmax(L), kmax(R)); a child c >= 0 is an internal node, c < 0 is leaf ~c.
+//   leaf  = 4 x float4: rows of the world->instance affine map [A | b] (A = diag(1/k) R^T,
+//           b = -A mu, k = kernel support scale per axis), then (gaussian id, kmax, 0, 0).
+struct AccelView {
+    const float4* nodes;
+    const float4* leaves;
+    const float4* bounds;  // [2]: scene AABB lo.xyz, hi.xyz (union of the instance AABBs)
+    int n;                 // number of Gaussians (leaves)
+};
+
+struct EnvView {
+    const float4* data;  // [h, w] RGBA texels, null when absent
+    int w, h;
+    int cube;            // 1 when h == 6 w
+    const float* prob;   // alias table [3, ah, aw]: prob, alias index (as float), pdf
+    const float* alias;
+    const float* pdf;
+    int aw, ah, cells;
+    float sin_z, cos_z, sin_x, cos_x;  // environment rotation (offset fixed at (0, 0))
+};
+
+enum Flags : unsigned {
+    kNormals = 1u,
+    kHitCounts = 2u,
+    kMis = 4u,
+    kMetallic = 8u,
+    kVisualizeLights = 16u,
+};
+
+struct ParticleView {
+    const float4* density;   // [n, 3] float4 = pos.xyz dns | quat wxyz | scale.xyz pad
+    const float* material;   // [n, 5]
+    const float* sph;        // [n, sph_stride]
+    const float* snrm;       // [n, 3] or null
+    int sph_stride;          // floats per particle (3 * max coefficients)
+    int sph_degree;          // evaluation degree (<= max)
+};
+
+struct TraceParams {
+    AccelView accel;
+    ParticleView part;
+    EnvView env;
+    const float* ray_to_world;   // [>=1, 4, 4] row-major; the first matrix applies to every ray
+    const float* ray_ori;        // [z, h, w, 3]
+    const float* ray_dir;
+    int nz, h, w;
+    unsigned frame;
+    unsigned flags;
+    int kernel_degree;
+    float min_response;          // hitMinGaussianResponse
+    float alpha_min;             // 1/255
+    float min_transmittance;
+    unsigned max_bounces;
+    unsigned render_opts;
+    int max_stack_overflows_unused;
+    unsigned* error_word;        // set on a bounded-loop violation (stack overflow, runaway loop)
+    unsigned long long* counters;  // [8]: segments, trace calls, candidates, accepted, env lookups, replay, -, -
+};
+
+struct FwdOutputs {
+    float* radiance;    // [z,h,w,3]
+    float* density;     // [z,h,w,1]
+    float* hit;         // [z,h,w,2]
+    float* hit2;        // [z,h,w,1]
+    float* distortion;  // [z,h,w,1]
+    float* normal;      // [z,h,w,3]
+    float* snormal;     // [z,h,w,3]
+    float* material;    // [z,h,w,5]
+    float* hits_count;  // [z,h,w,1]
+    float* pbr;         // [z,h,w,3]
+    float* light;       // [z,h,w,3]
+    float* components;  // [z,h,w,2,3]
+    float* visibility;  // [n] float32 tensor holding int32 1 where an accepted hit occurred
+};
+
+struct BwdInputs {
+    const float* pbr;            // [z,h,w,3]
+    const float* light;          // [z,h,w,3]
+    const float* pbr_grad;       // [z,h,w,3]
+    const float* light_grad;     // [z,h,w,3]
+    const float* material_grad;  // [z,h,w,5]
+    float* particle_material_grad;  // [n,5]
+    float* environment_grad;        // [eh,ew,4]
+};
+
+enum Counter : int {
+    kCtrSegments = 0,
+    kCtrTraceCalls = 1,
+    kCtrCandidates = 2,
+    kCtrAccepted = 3,
+    kCtrEnvLookups = 4,
+    kCtrReplay = 5,
+    kNumCounters = 8,
+};
+
+enum ErrorBits : unsigned {
+    kErrStackOverflow = 1u,
+    kErrLoopBound = 2u,
+};
+
+// launch helpers implemented in the .cu files
+cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, int block, cudaStream_t s);
+cudaError_t launch_trace_bwd(const TraceParams& p, const BwdInputs& b, int block, cudaStream_t s);
+
+}  // namespace ptir

@@ -1,0 +1,150 @@
+// Software LBVH traversal with a register k-buffer: the replacement for OptiX's
+// optixTrace + __intersection__is + __anyhit__ah of the reference
+// (threedgptir_tracer/include/3dgptir/kernels/cuda/pathTracer.cuh:58-113,
+//  src/kernels/cuda/referenceOptix.cu:73-133, gaussianParticles.cuh:484-500).
+//
+// One call returns the K candidates with the smallest closest-approach parameter t* in
+// (tmin, tend), ascending. A Gaussian is a candidate when its object-space ray hits the unit
+// instance box [-1,1]^3 within [tmin, tend] and passes the perpendicular-distance test.
+//
+// Pruning. Once the buffer is full, a subtree is skipped when its box entry exceeds
+// t_K + sqrt(3) kmax / |d|, where kmax bounds the kernel support of every Gaussian below it.
+// This is exact: for a candidate, |q(t)|^2 (q = object-space point) is a parabola in t with
+// curvature |d'|^2 >= |d|^2 / kmax^2 that is <= 3 somewhere inside the box, so
+// t* >= t_box_entry - sqrt(3) kmax / |d| >= t_node_entry - sqrt(3) kmax / |d|.
+#pragma once
+
+#include "device_types.h"
+#include "vecmath.cuh"
+
+namespace ptir {
+
+constexpr int kKBuf = 16;            // hits per trace call (reference MaxNumHitPerTrace)
+constexpr int kStackDepth = 64;      // traversal stack entries
+constexpr unsigned kNoHit = 0xFFFFFFFFu;
+constexpr float kFarT = 1e20f;
+
+struct TraceCounters {
+    unsigned segments, calls, candidates, accepted, env, replay;
+};
+
+PTIR_DEV void kbuf_clear(float (&kt)[kKBuf], unsigned (&kid)[kKBuf]) {
+#pragma unroll
+    for (int j = 0; j < kKBuf; ++j) {
+        kt[j] = kFarT;
+        kid[j] = kNoHit;
+    }
+}
+
+// number of filled slots
+PTIR_DEV unsigned kbuf_count(const unsigned (&kid)[kKBuf]) {
+    unsigned c = 0;
+#pragma unroll
+    for (int j = 0; j < kKBuf; ++j) c += kid[j] != kNoHit ? 1u : 0u;
+    return c;
+}
+
+// sorted insertion; an entry equal to an existing distance goes behind it
+PTIR_DEV void kbuf_insert(float (&kt)[kKBuf], unsigned (&kid)[kKBuf], float t, unsigned id) {
+#pragma unroll
+    for (int j = 0; j < kKBuf; ++j) {
+        const bool lt = t < kt[j];
+        const float tt = kt[j];
+        const unsigned ii = kid[j];
+        kt[j] = lt ? t : tt;
+        kid[j] = lt ? id : ii;
+        t = lt ? tt : t;
+        id = lt ? ii : id;
+    }
+}
+
+// ray vs AABB slab interval (inverse direction precomputed; NaNs from 0*inf are ignored by fmin/fmax)
+PTIR_DEV void slab(float3 lo, float3 hi, float3 o, float3 inv, float& t0, float& t1) {
+    const float ax = (lo.x - o.x) * inv.x, bx = (hi.x - o.x) * inv.x;
+    const float ay = (lo.y - o.y) * inv.y, by = (hi.y - o.y) * inv.y;
+    const float az = (lo.z - o.z) * inv.z, bz = (hi.z - o.z) * inv.z;
+    t0 = fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz));
+    t1 = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
+}
+
+// exact instance test of leaf record p
+PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[kKBuf],
+                        unsigned (&kid)[kKBuf]) {
+    const float4* rec = A.leaves + 4 * (size_t)p;
+    const float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
+    const float3 od = make_float3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w,
+                                  r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w,
+                                  r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
+    const float3 dd = make_float3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
+                                  r2.x * d.x + r2.y * d.y + r2.z * d.z);
+    const float dd2 = dot(dd, dd);
+    const float den = 1.0f / dd2;
+    const float ts = -dot(od, dd) * den;
+    if (!(ts > tmin && ts < tend && ts < kt[kKBuf - 1])) return;
+    // object-space unit box within [tmin, tend]
+    const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    float b0, b1;
+    slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
+    if (fmaxf(b0, tmin) > fminf(b1, tend)) return;
+    const float3 c = cross(normalize_or_keep(dd), od);
+    if (!(dot(c, c) * den < 9.0f)) return;
+    const unsigned gid = __float_as_uint(__ldg(&rec[3].x));
+    kbuf_insert(kt, kid, ts, gid);
+}
+
+// Fill (kt, kid) with the nearest candidates of ray (o, d) in (tmin, tend).
+PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[kKBuf],
+                         unsigned (&kid)[kKBuf], int* stack, unsigned* err, TraceCounters& ctr) {
+    kbuf_clear(kt, kid);
+    ++ctr.calls;
+    if (A.n <= 0) return;
+    if (A.n == 1) {
+        test_leaf(A, 0, o, d, tmin, tend, kt, kid);
+        ctr.candidates += kbuf_count(kid);
+        return;
+    }
+    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    const float margin = 1.7320508f * rsqrtf(dot(d, d));
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        const float4* nd = A.nodes + 4 * (size_t)node;
+        const float4 a = __ldg(nd + 0), b = __ldg(nd + 1), c = __ldg(nd + 2), e = __ldg(nd + 3);
+        const int left = __float_as_int(e.x), right = __float_as_int(e.y);
+        float l0, l1, r0, r1;
+        slab(make_float3(a.x, a.y, a.z), make_float3(a.w, b.x, b.y), o, inv, l0, l1);
+        slab(make_float3(b.z, b.w, c.x), make_float3(c.y, c.z, c.w), o, inv, r0, r1);
+        l0 = fmaxf(l0, tmin);
+        r0 = fmaxf(r0, tmin);
+        const float cut = kt[kKBuf - 1];
+        bool hl = l0 <= fminf(l1, tend) && l0 <= cut + margin * e.z;
+        bool hr = r0 <= fminf(r1, tend) && r0 <= cut + margin * e.w;
+        if (hl && left < 0) {
+            test_leaf(A, ~left, o, d, tmin, tend, kt, kid);
+            hl = false;
+        }
+        if (hr && right < 0) {
+            test_leaf(A, ~right, o, d, tmin, tend, kt, kid);
+            hr = false;
+        }
+        if (hl && hr) {
+            const bool lfirst = l0 <= r0;
+            if (sp >= kStackDepth) {
+                atomicOr(err, kErrStackOverflow);
+                break;
+            }
+            stack[sp++] = lfirst ? right : left;
+            node = lfirst ? left : right;
+        } else if (hl) {
+            node = left;
+        } else if (hr) {
+            node = right;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    ctr.candidates += kbuf_count(kid);
+}
+
+}  // namespace ptir

@@ -1,0 +1,248 @@
+"""``OptixTracer``: the native tracer object with the reference's pybind11 surface.
+
+Same constructor arguments and the same ``trace`` / ``trace_bwd`` / ``build_bvh`` methods,
+argument order, tensor layouts and return tuples as the reference class
+(threedgptir_tracer/bindings.cpp:32-38, include/3dgptir/optixTracer.h:130-217), backed by
+``libptir_b200.so`` through its C ABI instead of OptiX.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _native as N
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _f32(t: torch.Tensor, name: str) -> torch.Tensor:
+    """Contiguous float32 CUDA view of `t`; other dtypes are rejected like the reference's getPtr
+    (tensorBuffering.h:30-39)."""
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name}: expected a torch.Tensor")
+    if t.dtype != torch.float32:
+        raise TypeError(f"{name}: unsupported dtype {t.dtype} (float32 required)")
+    if not t.is_cuda:
+        raise ValueError(f"{name}: CUDA tensor required")
+    return t.contiguous()
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+class OptixTracer:
+    """Drop-in for ``libthreedgptir_cc.OptixTracer``."""
+
+    def __init__(
+        self,
+        path: str,
+        cuda_path: str,
+        pipeline: str,
+        backward_pipeline: str,
+        primitive: str,
+        particle_kernel_degree: float,
+        particle_kernel_min_response: float,
+        particle_kernel_density_clamping: bool,
+        particle_radiance_sph_degree: int,
+        enable_normals: bool,
+        enable_hit_counts: bool,
+        enable_mis: bool,
+        enable_metallic: bool,
+        visualize_lights: bool = False,
+        collect_counters: bool = True,
+    ):
+        if pipeline not in ("reference",):
+            raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
+        if backward_pipeline not in ("referenceBwd",):
+            raise ValueError(f"backward pipeline '{backward_pipeline}' is not available (only 'referenceBwd')")
+        if primitive not in ("instances",):
+            raise ValueError(f"primitive type '{primitive}' is not available (only 'instances')")
+        self._lib = N.load()
+        self.sph_degree = int(particle_radiance_sph_degree)
+        self.enable_normals = bool(enable_normals)
+        cfg = N.PtirConfig(
+            float(particle_kernel_degree), float(particle_kernel_min_response), int(bool(particle_kernel_density_clamping)),
+            self.sph_degree, int(bool(enable_normals)), int(bool(enable_hit_counts)), int(bool(enable_mis)),
+            int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)))
+        handle = C.c_void_p()
+        rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
+        if rc != N.PTIR_OK:
+            raise N.PtirError(rc, "ptir_create failed (check the construction options)")
+        self._h = handle
+        self._n = -1
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.ptir_destroy(h)
+            self._h = None
+
+    # --------------------------------------------------------------------------------
+    def build_bvh(self, mog_pos, mog_rot, mog_scl, mog_dns, rebuild, allow_update=True):
+        """buildBVH (optixTracer.cpp:633-907): instance boxes -> LBVH (rebuild) or refit."""
+        pos, rot = _f32(mog_pos, "mog_pos"), _f32(mog_rot, "mog_rot")
+        scl, dns = _f32(mog_scl, "mog_scl"), _f32(mog_dns, "mog_dns")
+        n = pos.shape[0]
+        if rot.shape != (n, 4) or scl.shape != (n, 3) or dns.numel() != n:
+            raise ValueError("build_bvh: expected pos [N,3], rot [N,4], scl [N,3], dns [N,1]")
+        rc = self._lib.ptir_build_bvh(self._h, _ptr(pos), _ptr(rot), _ptr(scl), _ptr(dns), int(n), int(bool(rebuild)),
+                                      int(bool(allow_update)), _stream())
+        N.check(self._h, rc, "build_bvh")
+        self._n = n
+
+    # --------------------------------------------------------------------------------
+    def _args(self, frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material, particle_radiance,
+              particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
+              mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table, sh_indirect,
+              sph_degree, min_transmittance, max_bounces):
+        keep = []
+        t2w = _f32(ray_to_world, "ray_to_world")
+        if t2w.numel() < 12:
+            raise ValueError("ray_to_world must hold at least one 3x4 (or 4x4) transform")
+        ori, dirs = _f32(ray_ori, "ray_ori"), _f32(ray_dir, "ray_dir")
+        if ori.dim() != 4 or ori.shape[-1] != 3 or dirs.shape != ori.shape:
+            raise ValueError("ray_ori / ray_dir must be [Z,H,W,3]")
+        dens = _f32(particle_density, "particle_density")
+        mat = _f32(particle_material, "particle_material")
+        rad = _f32(particle_radiance, "particle_radiance")
+        n = dens.shape[0]
+        if dens.shape != (n, 12) or mat.shape != (n, 5):
+            raise ValueError("particle_density must be [N,12] and particle_material [N,5]")
+        coeffs = (self.sph_degree + 1) ** 2 * 3
+        if rad.shape != (n, coeffs):
+            raise ValueError(f"particle_radiance must be [N,{coeffs}]")
+        snrm = _f32(particle_shading_normal, "particle_shading_normal") if particle_shading_normal is not None else None
+        if snrm is not None and snrm.numel() != 3 * n:
+            raise ValueError("particle_shading_normal must be [N,3]")
+        env = environment
+        env_ok = (isinstance(env, torch.Tensor) and env.dim() >= 3 and env.shape[0] > 0 and env.shape[1] > 0
+                  and env.shape[2] == 4 and env.numel() > 0)
+        env = _f32(env, "environment") if env_ok else None
+        alias = environment_alias_table
+        alias_ok = (isinstance(alias, torch.Tensor) and alias.dim() == 3 and alias.shape[0] == 3 and alias.shape[1] > 0
+                    and alias.shape[2] > 0)
+        alias = _f32(alias, "environment_alias_table") if alias_ok else None
+        n_lights = int(lights.shape[0]) if lights is not None else 0
+        n_entries = int(light_alias_table.shape[1]) if light_alias_table is not None and light_alias_table.dim() == 2 else 0
+        n_mesh = int(mesh_lights.shape[0]) if mesh_lights is not None else 0
+        keep += [t2w, ori, dirs, dens, mat, rad, snrm, env, alias]
+        a = N.PtirTraceArgs()
+        a.frame = int(frame) & 0xFFFFFFFF
+        a.ray_to_world = _ptr(t2w)
+        a.ray_origin, a.ray_direction = _ptr(ori), _ptr(dirs)
+        a.z, a.h, a.w = int(ori.shape[0]), int(ori.shape[1]), int(ori.shape[2])
+        a.particle_density, a.particle_material, a.particle_radiance = _ptr(dens), _ptr(mat), _ptr(rad)
+        a.particle_shading_normal = _ptr(snrm)
+        a.n = int(n)
+        a.environment = _ptr(env)
+        a.env_h, a.env_w = (int(env.shape[0]), int(env.shape[1])) if env is not None else (0, 0)
+        a.environment_alias = _ptr(alias)
+        a.alias_h, a.alias_w = (int(alias.shape[1]), int(alias.shape[2])) if alias is not None else (0, 0)
+        a.num_lights, a.num_light_entries, a.num_mesh_lights = n_lights, n_entries, n_mesh
+        a.sh_indirect = int(sh_indirect)
+        a.sph_eval_degree = int(sph_degree)
+        a.min_transmittance = float(min_transmittance)
+        a.max_bounces = int(max_bounces)
+        return a, keep, ori.shape[:3], n, env
+
+    def trace(self, frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material, particle_radiance,
+              particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
+              mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table, sh_indirect,
+              sph_degree, min_transmittance, max_bounces):
+        """trace (optixTracer.cpp:909-1013). Returns (rayRad, rayDns, rayHit[...,2], rayHitSecondMoment,
+        rayDepthDistortion, rayNrm, rayShadingNrm, rayMaterial, rayHitsCount, particleVisibility, rayPbr,
+        rayLight, rayPbrComponents)."""
+        a, keep, zhw, n, _ = self._args(frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material,
+                                        particle_radiance, particle_shading_normal, environment, environment_alias_table,
+                                        lights, light_alias_table, mesh_light_vertices, mesh_light_triangles,
+                                        mesh_lights, mesh_light_triangle_alias_table, sh_indirect, sph_degree,
+                                        min_transmittance, max_bounces)
+        dev = particle_density.device
+        e = lambda c: torch.empty((*zhw, c), dtype=torch.float32, device=dev)  # noqa: E731
+        out = dict(radiance=e(3), density=e(1), hit=e(2), hit2=e(1), distortion=e(1), normal=e(3), snormal=e(3),
+                   material=e(5), hits=e(1))
+        vis = torch.empty((n, 1), dtype=torch.float32, device=dev)
+        pbr, light = e(3), e(3)
+        comps = torch.empty((*zhw, 2, 3), dtype=torch.float32, device=dev)
+        o = N.PtirTraceOutputs(
+            _ptr(out["radiance"]), _ptr(out["density"]), _ptr(out["hit"]), _ptr(out["hit2"]), _ptr(out["distortion"]),
+            _ptr(out["normal"]), _ptr(out["snormal"]), _ptr(out["material"]), _ptr(out["hits"]), _ptr(pbr),
+            _ptr(light), _ptr(comps), _ptr(vis))
+        rc = self._lib.ptir_trace(self._h, C.byref(a), C.byref(o), _stream())
+        N.check(self._h, rc, "trace")
+        del keep
+        return (out["radiance"], out["density"], out["hit"], out["hit2"], out["distortion"], out["normal"],
+                out["snormal"], out["material"], out["hits"], vis, pbr, light, comps)
+
+    def trace_bwd(self, frame, ray_to_world, ray_ori, ray_dir, ray_rad, ray_dns, ray_hit, ray_hit_second_moment,
+                  ray_depth_distortion, ray_nrm, ray_shading_nrm, ray_material, ray_pbr, ray_light, particle_density,
+                  particle_material, particle_radiance, particle_shading_normal, environment, environment_alias_table,
+                  lights, light_alias_table, mesh_light_vertices, mesh_light_triangles, mesh_lights,
+                  mesh_light_triangle_alias_table, ray_rad_grd, ray_dns_grd, ray_hit_grd, ray_hit_second_moment_grd,
+                  ray_depth_distortion_grd, ray_nrm_grd, ray_shading_nrm_grd, ray_material_grd, ray_pbr_grd,
+                  ray_light_grd, sh_indirect, sph_degree, min_transmittance, max_bounces):
+        """traceBwd (optixTracer.cpp:1015-1145). Returns (densityGrad [N,12], materialGrad [N,5],
+        radianceGrad [N,C], shadingNormalGrad [N,3], environmentGrad like environment); as in the
+        reference only the material and environment gradients are non-zero."""
+        a, keep, zhw, n, env = self._args(frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material,
+                                          particle_radiance, particle_shading_normal, environment,
+                                          environment_alias_table, lights, light_alias_table, mesh_light_vertices,
+                                          mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table,
+                                          sh_indirect, sph_degree, min_transmittance, max_bounces)
+        dev = particle_density.device
+
+        def g(t, c, name):
+            if t is None:
+                return None
+            t = _f32(t, name)
+            if tuple(t.shape[:3]) != tuple(zhw) or t.shape[-1] != c:
+                raise ValueError(f"{name} must be [Z,H,W,{c}]")
+            return t
+
+        pbr, light = g(ray_pbr, 3, "ray_pbr"), g(ray_light, 3, "ray_light")
+        pbr_g, light_g = g(ray_pbr_grd, 3, "ray_pbr_grd"), g(ray_light_grd, 3, "ray_light_grd")
+        mat_g = g(ray_material_grd, 5, "ray_material_grd")
+        keep += [pbr, light, pbr_g, light_g, mat_g]
+        density_grad = torch.zeros((n, 12), dtype=torch.float32, device=dev)
+        material_grad = torch.empty((n, 5), dtype=torch.float32, device=dev)
+        radiance_grad = torch.zeros_like(particle_radiance)
+        snrm_grad = (torch.zeros_like(particle_shading_normal) if particle_shading_normal is not None
+                     else torch.zeros((n, 3), dtype=torch.float32, device=dev))
+        env_grad = torch.zeros_like(environment)
+        b = N.PtirBwdArgs(_ptr(pbr), _ptr(light), _ptr(pbr_g), _ptr(light_g), _ptr(mat_g))
+        o = N.PtirBwdOutputs(_ptr(material_grad), _ptr(env_grad) if env is not None else None)
+        rc = self._lib.ptir_trace_bwd(self._h, C.byref(a), C.byref(b), C.byref(o), _stream())
+        N.check(self._h, rc, "trace_bwd")
+        del keep
+        return density_grad, material_grad, radiance_grad, snrm_grad, env_grad
+
+    # --------------------------------------------------------------------------------
+    # extensions (not in the reference): counters and device status for tests and benchmarks
+    def counters(self) -> dict:
+        c = N.PtirCounters()
+        N.check(self._h, self._lib.ptir_get_counters(self._h, C.byref(c), _stream()), "counters")
+        return c.as_dict()
+
+    def device_status(self) -> int:
+        w = C.c_uint32(0)
+        self._lib.ptir_device_status(self._h, C.byref(w), _stream())
+        return int(w.value)
+
+    def scene_bounds(self) -> torch.Tensor:
+        out = (C.c_float * 6)()
+        N.check(self._h, self._lib.ptir_scene_bounds(self._h, out, _stream()), "scene_bounds")
+        return torch.tensor(list(out), dtype=torch.float32)
+
+    def debug_accel(self):
+        """(nodes [N-1,16], leaves [N,16]) float32 host copies of the acceleration structure."""
+        n = max(self._n, 0)
+        nodes = torch.zeros((max(n - 1, 0), 16), dtype=torch.float32)
+        leaves = torch.zeros((n, 16), dtype=torch.float32)
+        rc = self._lib.ptir_debug_accel(self._h, nodes.data_ptr() if n > 1 else None, leaves.data_ptr() if n else None,
+                                        _stream())
+        N.check(self._h, rc, "debug_accel")
+        return nodes, leaves

@@ -1,0 +1,82 @@
+"""Small seeded scenes shared by the oracle and GPU tests."""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from ptir_b200 import envmap, synthetic
+
+
+def small_scene(n=2000, w=48, h=40, spp=1, views=1, max_bounces=3, env_hw=(32, 64), seed=0, sh_full=False,
+                scale_range=(0.01, 0.08), frame=3, sh_degree=3, env=True, alias=True, cube=False, layout="uniform"):
+    """Returns a dict of numpy float32 arrays in the tracer's layouts plus the scalars, ready for
+    oracle.trace() and for to_torch()."""
+    f = synthetic.make_field(n, seed=seed, layout=layout, scale_range=scale_range, sh_degree=sh_degree, sh_full=sh_full)
+    eyes = synthetic.camera_positions(views, seed=seed)
+    oris, dirs = [], []
+    for v in range(views):
+        o, d = synthetic.view_rays(w, h, spp, eyes[v])
+        oris.append(o)
+        dirs.append(d)
+    # launch z = sample * views + view (the reference's spp expansion order)
+    ori = torch.stack(oris, 1).reshape(spp * views, h, w, 3)
+    dr = torch.stack(dirs, 1).reshape(spp * views, h, w, 3)
+    s = dict(
+        build_pos=f["pos"].numpy(), build_rot=f["rot"].numpy(), build_scl=f["scl"].numpy(), build_dns=f["dns"].numpy(),
+        density=synthetic.density_tensor(f).numpy(), material=synthetic.material_tensor(f).numpy(),
+        sph=f["sph"].numpy(), shading_normal=f["snrm"].numpy(),
+        ray_ori=ori.numpy(), ray_dir=dr.numpy(), ray_to_world=np.eye(4, dtype=np.float32)[None],
+        frame=frame, sph_degree=sh_degree, min_transmittance=0.001, max_bounces=max_bounces, render_opts=0,
+    )
+    if env:
+        eh, ew = env_hw
+        e = synthetic.make_environment(6 * ew if cube else eh, ew, seed=seed)
+        s["environment"] = e.numpy()
+        if alias:
+            s["alias_table"] = envmap.pack(envmap.build(e, cube=cube)).numpy()
+        else:
+            s["alias_table"] = np.zeros((0,), np.float32)
+    else:
+        s["environment"] = np.zeros((0, 0, 4), np.float32)
+        s["alias_table"] = np.zeros((0,), np.float32)
+    return s
+
+
+def to_torch(s: dict, device="cuda") -> dict:
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
+    return {k: (t(v) if isinstance(v, np.ndarray) else v) for k, v in s.items()}
+
+
+def make_tracer(sph_degree=3, normals=True, hitcounts=True, mis=True, metallic=False, visualize=False,
+                kernel_degree=4, min_response=0.0113, clamping=True):
+    from ptir_b200 import OptixTracer
+
+    return OptixTracer("", "", "reference", "referenceBwd", "instances", kernel_degree, min_response, clamping,
+                       sph_degree, normals, hitcounts, mis, metallic, visualize)
+
+
+def gpu_trace(tr, S: dict, build=True, rebuild=True):
+    """Run build_bvh + trace on torch CUDA scene S (from to_torch). Returns the 13-tuple."""
+    empty = lambda *shape, dt=torch.float32: torch.empty(shape, dtype=dt, device=S["density"].device)  # noqa: E731
+    if build:
+        tr.build_bvh(S["build_pos"], S["build_rot"], S["build_scl"], S["build_dns"], rebuild, True)
+    return tr.trace(S["frame"], S["ray_to_world"], S["ray_ori"], S["ray_dir"], S["density"], S["material"], S["sph"],
+                    S["shading_normal"], S["environment"], S["alias_table"], empty(0, 9), empty(5, 0), empty(0, 3),
+                    empty(0, 3, dt=torch.int32), empty(0, 8), empty(3, 0), S["render_opts"], S["sph_degree"],
+                    S["min_transmittance"], S["max_bounces"])
+
+
+def gpu_trace_bwd(tr, S: dict, fwd, pbr_grad, light_grad=None, material_grad=None):
+    empty = lambda *shape, dt=torch.float32: torch.empty(shape, dtype=dt, device=S["density"].device)  # noqa: E731
+    (rad, dns, hit, hit2, dist, nrm, snrm, mat, hits, vis, pbr, light, comps) = fwd
+    z = lambda t: torch.zeros_like(t)  # noqa: E731
+    if light_grad is None:
+        light_grad = z(light)
+    if material_grad is None:
+        material_grad = z(mat)
+    return tr.trace_bwd(S["frame"], S["ray_to_world"], S["ray_ori"], S["ray_dir"], rad, dns, hit, hit2, dist, nrm, snrm,
+                        mat, pbr, light, S["density"], S["material"], S["sph"], S["shading_normal"], S["environment"],
+                        S["alias_table"], empty(0, 9), empty(5, 0), empty(0, 3), empty(0, 3, dt=torch.int32),
+                        empty(0, 8), empty(3, 0), z(rad), z(dns), z(hit), z(hit2), z(dist), z(nrm), z(snrm),
+                        material_grad, pbr_grad, light_grad, S["render_opts"], S["sph_degree"], S["min_transmittance"],
+                        S["max_bounces"])

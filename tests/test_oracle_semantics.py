@@ -1,0 +1,83 @@
+"""The oracle's candidate gathering equals brute force, and its two precisions agree."""
+import numpy as np
+
+from oracle import oracle as O
+from tests.scenes import small_scene
+
+
+def _brute_force(s, cfg, ray, tmin, tend):
+    """Order-independent candidate set of one trace call, straight from the definitions
+    (unit instance box hit within [tmin, tend], tmin < t* < tend, perp^2/|d'|^2 < 9)."""
+    aabb, ks, _, _ = O.instances(cfg, s)
+    pos, rot, scl = (s["build_pos"].astype(np.float64), s["build_rot"].astype(np.float64),
+                     s["build_scl"].astype(np.float64))
+    o, d = ray[:3].astype(np.float64), ray[3:].astype(np.float64)
+    hits = []
+    for g in range(pos.shape[0]):
+        w, x, y, z = rot[g]
+        R = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                      [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                      [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+        k = scl[g] * ks[g]
+        A = (R.T) / k[:, None]
+        oo, dd = A @ (o - pos[g]), A @ d
+        te, tx = tmin, tend
+        miss = False
+        for a in range(3):
+            if dd[a] == 0:
+                miss |= abs(oo[a]) > 1
+                continue
+            t0, t1 = sorted(((-1 - oo[a]) / dd[a], (1 - oo[a]) / dd[a]))
+            te, tx = max(te, t0), min(tx, t1)
+        if miss or te > tx:
+            continue
+        ts = -oo @ dd / (dd @ dd)
+        if not (tmin < ts < tend):
+            continue
+        c = np.cross(dd / np.linalg.norm(dd), oo)
+        if c @ c / (dd @ dd) < 9:
+            hits.append((ts, g))
+    hits.sort()
+    return hits[:16]
+
+
+def test_candidates_equal_brute_force():
+    cfg = O.OracleConfig()
+    s = small_scene(n=400, w=8, h=8, scale_range=(0.02, 0.2))
+    rng = np.random.default_rng(0)
+    m = 24
+    o = rng.uniform(-1.5, 1.5, (m, 3))
+    d = rng.standard_normal((m, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = np.concatenate([o, d], 1).astype(np.float32)
+    tmin = rng.uniform(0.0, 0.5, m).astype(np.float32)
+    tend = (tmin + rng.uniform(0.5, 4.0, m)).astype(np.float32)
+    ids, ts = O.candidates(cfg, s, rays, tmin, tend)
+    for i in range(m):
+        bf = _brute_force(s, cfg, rays[i], float(tmin[i]), float(tend[i]))
+        got = [(t, int(g)) for t, g in zip(ts[i], ids[i]) if g != 0xFFFFFFFF]
+        assert [g for _, g in got] == [g for _, g in bf], i
+        assert np.allclose([t for t, _ in got], [t for t, _ in bf], rtol=1e-9)
+
+
+def test_f32_and_f64_oracles_agree():
+    s = small_scene(n=1500, w=32, h=24, spp=2)
+    cfg = O.OracleConfig()
+    a, va, sa = O.trace(cfg, s, "f64")
+    b, vb, sb = O.trace(cfg, s, "f32")
+    for k in ("radiance", "density", "material"):
+        close = np.all(np.abs(a[k] - b[k]) <= 1e-3 + 1e-3 * np.abs(a[k]), axis=-1)
+        assert close.mean() >= 0.995, k
+    assert abs(sa.segments - sb.segments) <= 0.01 * sa.segments
+
+
+def test_stride_sampling_is_a_subset():
+    """The bounded CPU-baseline sample (every k-th launch) renders those launches identically."""
+    s = small_scene(n=800, w=16, h=16)
+    cfg = O.OracleConfig()
+    full, _, _ = O.trace(cfg, s, "f32")
+    part, _, st = O.trace(cfg, s, "f32", stride=5)
+    flat_f = full["radiance"].reshape(-1, 3)
+    flat_p = part["radiance"].reshape(-1, 3)
+    assert np.array_equal(flat_f[::5], flat_p[::5])
+    assert st.segments > 0
