@@ -128,12 +128,16 @@ typedef struct ptir_bwd_outputs {
 
 /* Device counters of the most recent trace / trace_bwd (collect_counters = 1). */
 typedef struct ptir_counters {
-    uint64_t segments;      /* rays traced through the field: primary, shadow and bounce rays */
-    uint64_t trace_calls;   /* k-buffer traversals */
-    uint64_t candidates;    /* candidates returned by the traversals */
-    uint64_t accepted;      /* hits composited */
-    uint64_t env_lookups;   /* bilinear environment lookups */
-    uint64_t replay;        /* backward re-traversals of a segment */
+    uint64_t segments;        /* rays traced through the field: primary, shadow and bounce rays
+                                 (the backward counts its replay of the forward path the same way) */
+    uint64_t trace_calls;     /* k-buffer traversals */
+    uint64_t candidates;      /* candidates returned by the traversals */
+    uint64_t accepted;        /* hits composited by primary / bounce segments */
+    uint64_t env_lookups;     /* bilinear environment lookups */
+    uint64_t replay;          /* backward re-traversals of a segment that scatter material gradients */
+    uint64_t replay_accepted; /* hits that received a material gradient */
+    uint64_t node_visits;     /* internal BVH nodes fetched (implementation overhead) */
+    uint64_t leaf_tests;      /* exact instance tests */
 } ptir_counters;
 
 int ptir_abi_version(void);

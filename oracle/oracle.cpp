@@ -1304,7 +1304,7 @@ static int run_fwd(const orc_config* c, const orc_scene* s, const orc_fwd_out* o
 
 template <class T>
 static int run_bwd(const orc_config* c, const orc_scene* s, const orc_bwd_in* b, double* mat_grad, double* env_grad,
-                   int nthreads, orc_stats* stats) {
+                   int nthreads, long long stride, orc_stats* stats) {
     const Config cfg = to_cfg(c);
     const Inputs in = to_in(s);
     Instances<T> I;
@@ -1313,6 +1313,7 @@ static int run_bwd(const orc_config* c, const orc_scene* s, const orc_bwd_in* b,
     bi.pbr = b->pbr; bi.light = b->light; bi.pbr_grad = b->pbr_grad; bi.light_grad = b->light_grad;
     bi.material_grad = b->material_grad;
     const long long total = (long long)in.nz * in.h * in.w;
+    if (stride < 1) stride = 1;
     if (nthreads > 0) omp_set_num_threads(nthreads);
     const int nt = omp_get_max_threads();
     std::vector<std::vector<double>> mg(nt), eg(nt);
@@ -1326,7 +1327,7 @@ static int run_bwd(const orc_config* c, const orc_scene* s, const orc_bwd_in* b,
         tr.mat_grad = &mg[t];
         tr.env_grad = &eg[t];
 #pragma omp for schedule(dynamic, 64)
-        for (long long li = 0; li < total; ++li) {
+        for (long long li = 0; li < total; li += stride) {
             const uint32_t x = uint32_t(li % in.w), y = uint32_t((li / in.w) % in.h), z = uint32_t(li / ((long long)in.w * in.h));
             tr.backward_one(size_t(li), x, y, z, bi);
         }
@@ -1356,11 +1357,11 @@ int orc_trace_f32(const orc_config* c, const orc_scene* s, const orc_fwd_out* o,
 }
 int orc_trace_bwd_f64(const orc_config* c, const orc_scene* s, const orc_bwd_in* b, double* mat_grad, double* env_grad,
                       int nthreads, orc_stats* stats) {
-    return run_bwd<double>(c, s, b, mat_grad, env_grad, nthreads, stats);
+    return run_bwd<double>(c, s, b, mat_grad, env_grad, nthreads, 1, stats);
 }
 int orc_trace_bwd_f32(const orc_config* c, const orc_scene* s, const orc_bwd_in* b, double* mat_grad, double* env_grad,
-                      int nthreads, orc_stats* stats) {
-    return run_bwd<float>(c, s, b, mat_grad, env_grad, nthreads, stats);
+                      int nthreads, long long stride, orc_stats* stats) {
+    return run_bwd<float>(c, s, b, mat_grad, env_grad, nthreads, stride, stats);
 }
 
 // candidate lists of single trace() calls, for traversal tests: rays [m,6] (o,d), tmin/tend [m];

@@ -93,7 +93,8 @@ def lib():
         L.orc_trace_f64.argtypes = [P(_Config), P(_Scene), P(_FwdOut), C.c_int, P(Stats)]
         L.orc_trace_f32.argtypes = [P(_Config), P(_Scene), P(_FwdOut), C.c_int, C.c_longlong, P(Stats)]
         L.orc_trace_bwd_f64.argtypes = [P(_Config), P(_Scene), P(_BwdIn), P(C.c_double), P(C.c_double), C.c_int, P(Stats)]
-        L.orc_trace_bwd_f32.argtypes = [P(_Config), P(_Scene), P(_BwdIn), P(C.c_double), P(C.c_double), C.c_int, P(Stats)]
+        L.orc_trace_bwd_f32.argtypes = [P(_Config), P(_Scene), P(_BwdIn), P(C.c_double), P(C.c_double), C.c_int,
+                                        C.c_longlong, P(Stats)]
         L.orc_trace_candidates.argtypes = [P(_Config), P(_Scene), C.c_int, _FP, _FP, _FP, P(C.c_uint), P(C.c_double)]
         L.orc_instances.argtypes = [P(_Config), P(_Scene), P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double)]
         L.orc_sampler_stream.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.c_uint, C.c_int, P(C.c_uint)]
@@ -214,7 +215,8 @@ def trace(cfg: OracleConfig, scene: dict, precision: str = "f64", threads: int =
     return outs, vis[: sc.n], st
 
 
-def trace_bwd(cfg: OracleConfig, scene: dict, fwd: dict, grads: dict, precision: str = "f64", threads: int = 0):
+def trace_bwd(cfg: OracleConfig, scene: dict, fwd: dict, grads: dict, precision: str = "f64", threads: int = 0,
+              stride: int = 1):
     """Backward (path replay). ``fwd`` holds 'pbr' and 'light'; ``grads`` holds 'pbr', 'light',
     'material' output gradients. Returns (material_grad [n,5] f64, env_grad [eh,ew,4] f64, Stats)."""
     keep = _Keep()
@@ -225,9 +227,14 @@ def trace_bwd(cfg: OracleConfig, scene: dict, fwd: dict, grads: dict, precision:
     eg = np.zeros((max(sc.eh, 1), max(sc.ew, 1), 4), np.float64)
     st = Stats()
     c = cfg._c()
-    fn = lib().orc_trace_bwd_f64 if precision == "f64" else lib().orc_trace_bwd_f32
-    rc = fn(C.byref(c), C.byref(sc), C.byref(bi), mg.ctypes.data_as(C.POINTER(C.c_double)),
-            eg.ctypes.data_as(C.POINTER(C.c_double)), threads, C.byref(st))
+    P = C.POINTER(C.c_double)
+    if precision == "f64":
+        assert stride == 1
+        rc = lib().orc_trace_bwd_f64(C.byref(c), C.byref(sc), C.byref(bi), mg.ctypes.data_as(P), eg.ctypes.data_as(P),
+                                     threads, C.byref(st))
+    else:
+        rc = lib().orc_trace_bwd_f32(C.byref(c), C.byref(sc), C.byref(bi), mg.ctypes.data_as(P), eg.ctypes.data_as(P),
+                                     threads, stride, C.byref(st))
     assert rc == 0
     return mg[: sc.n], eg[: sc.eh, : sc.ew], st
 

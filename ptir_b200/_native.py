@@ -74,7 +74,8 @@ class PtirBwdOutputs(C.Structure):
 
 
 class PtirCounters(C.Structure):
-    _fields_ = [(k, C.c_uint64) for k in ("segments", "trace_calls", "candidates", "accepted", "env_lookups", "replay")]
+    _fields_ = [(k, C.c_uint64) for k in ("segments", "trace_calls", "candidates", "accepted", "env_lookups", "replay",
+                                          "replay_accepted", "node_visits", "leaf_tests")]
 
     def as_dict(self) -> dict:
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

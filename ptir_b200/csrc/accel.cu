@@ -3,7 +3,7 @@
 //
 //   1. prep      per Gaussian: kernel support scale, world->instance map, instance AABB
 //                (the instance transform of threedgptir_tracer/src/particlePrimitives.cu:543-610)
-//   2. bounds    scene AABB (two-pass reduction)
+//   2. bounds    scene AABB = union of the instance AABBs (two-pass reduction)
 //   3. morton    63-bit Morton key of the AABB centre within the scene bounds
 //   4. sort      key/id radix sort (CUB)
 //   5. gather    leaf records in key order
@@ -56,7 +56,7 @@ __global__ void k_prep(int n, const float* __restrict__ pos, const float* __rest
     rec[1] = make_float4(a1.x, a1.y, a1.z, -dot(a1, mu));
     rec[2] = make_float4(a2.x, a2.y, a2.z, -dot(a2, mu));
     rec[3] = make_float4(__uint_as_float((unsigned)g), kmax, 0.0f, 0.0f);
-    // AABB of the 8 transformed corners of [-1,1]^3
+    // AABB of the 8 transformed corners of [-1,1]^3 (particlePrimitives.cu:585-594)
     float3 lo = f3(3.0e38f), hi = f3(-3.0e38f);
 #pragma unroll
     for (int c = 0; c < 8; ++c) {

@@ -253,6 +253,9 @@ int ptir_get_counters(ptir_tracer* t, ptir_counters* out, void* stream) {
     out->accepted = h[ptir::kCtrAccepted];
     out->env_lookups = h[ptir::kCtrEnvLookups];
     out->replay = h[ptir::kCtrReplay];
+    out->replay_accepted = h[ptir::kCtrReplayAccepted];
+    out->node_visits = h[ptir::kCtrNodes];
+    out->leaf_tests = h[ptir::kCtrLeaves];
     return PTIR_OK;
 }
 

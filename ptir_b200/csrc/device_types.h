@@ -65,9 +65,9 @@ struct TraceParams {
     float min_transmittance;
     unsigned max_bounces;
     unsigned render_opts;
-    int max_stack_overflows_unused;
     unsigned* error_word;        // set on a bounded-loop violation (stack overflow, runaway loop)
-    unsigned long long* counters;  // [8]: segments, trace calls, candidates, accepted, env lookups, replay, -, -
+    unsigned long long* counters;  // [kNumCounters] indexed by Counter
+
 };
 
 struct FwdOutputs {
@@ -103,7 +103,10 @@ enum Counter : int {
     kCtrAccepted = 3,
     kCtrEnvLookups = 4,
     kCtrReplay = 5,
-    kNumCounters = 8,
+    kCtrReplayAccepted = 6,
+    kCtrNodes = 7,
+    kCtrLeaves = 8,
+    kNumCounters = 10,
 };
 
 enum ErrorBits : unsigned {

@@ -63,6 +63,7 @@ struct PathState {
 struct Ctx {
     const TraceParams& P;
     int* stack;
+    float* stack_t;
     TraceCounters& ctr;
 };
 
@@ -162,7 +163,7 @@ PTIR_DEV bool shadow_occluded(const Ctx& C, float3 o, float3 d, Pcg32& rng) {
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
-        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, P.error_word, C.ctr);
+        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
         float batch_end = start;
         bool stop = false;
@@ -337,9 +338,10 @@ PTIR_DEV bool launch_index(const TraceParams& P, unsigned& x, unsigned& y, unsig
 
 PTIR_DEV void flush_counters(const TraceParams& P, const TraceCounters& c) {
     if (P.counters == nullptr) return;
-    const unsigned v[6] = {c.segments, c.calls, c.candidates, c.accepted, c.env, c.replay};
+    const unsigned v[9] = {c.segments, c.calls, c.candidates, c.accepted, c.env, c.replay, c.replay_accepted, c.nodes,
+                           c.leaves};
 #pragma unroll
-    for (int k = 0; k < 6; ++k) {
+    for (int k = 0; k < 9; ++k) {
         const unsigned s = __reduce_add_sync(0xFFFFFFFFu, v[k]);
         if ((threadIdx.x & 31u) == 0u && s) atomicAdd(P.counters + k, (unsigned long long)s);
     }
@@ -352,8 +354,9 @@ PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis);
 
 __global__ void __launch_bounds__(128) k_trace_fwd(TraceParams P, FwdOutputs O) {
     int stack[kStackDepth];
-    TraceCounters ctr = {0, 0, 0, 0, 0, 0};
-    Ctx C{P, stack, ctr};
+    float stack_t[kStackDepth];
+    TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    Ctx C{P, stack, stack_t, ctr};
     unsigned x, y, z;
     if (launch_index(P, x, y, z)) {
         const size_t li = ((size_t)z * P.h + y) * P.w + x;
@@ -433,7 +436,7 @@ PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
-        trace_kbuf(P.accel, s.o, s.d, s.last_hit + 1e-9f, clip.y + 1e-9f, kt, kid, C.stack, P.error_word, C.ctr);
+        trace_kbuf(P.accel, s.o, s.d, s.last_hit + 1e-9f, clip.y + 1e-9f, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
 #pragma unroll
         for (int i = 0; i < kKBuf; ++i) {
@@ -511,7 +514,7 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, bool self_o
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
-        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, P.error_word, C.ctr);
+        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
 #pragma unroll
         for (int i = 0; i < kKBuf; ++i) {
@@ -524,6 +527,7 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, bool self_o
             float dns;
             const Response r = respond(P, id, o, d, dns);
             if (r.gres > P.min_response && r.alpha > P.alpha_min) {
+                ++C.ctr.replay_accepted;
                 const float w = r.alpha * tr;
                 float* g = B.particle_material_grad + 5 * (size_t)id;
                 atomicAdd(g + 0, w * da.x);
@@ -696,8 +700,9 @@ PTIR_DEV void sample_next_bwd(const Ctx& C, const BwdInputs& B, PathState& ps, S
 
 __global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
     int stack[kStackDepth];
-    TraceCounters ctr = {0, 0, 0, 0, 0, 0};
-    Ctx C{P, stack, ctr};
+    float stack_t[kStackDepth];
+    TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    Ctx C{P, stack, stack_t, ctr};
     unsigned x, y, z;
     if (launch_index(P, x, y, z)) {
         const size_t li = ((size_t)z * P.h + y) * P.w + x;
@@ -713,6 +718,7 @@ __global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
         float3 o, d;
         world_ray(P, li, o, d);
         segment_reset(s, o, d, 0.0f);
+        ++ctr.segments;
         intersect_mark<false>(C, s, rng, nullptr);
         if (s.ivalid && B.material_grad) {
             const float* mg = B.material_grad + 5 * li;
@@ -730,6 +736,7 @@ __global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
                 ps.bounces = depth + 1u;
                 sample_next_bwd(C, B, ps, s, rng);
                 if (max3(ps.throughput) < 1e-4f) break;
+                ++ctr.segments;
                 intersect_mark<true>(C, s, rng, nullptr);
             }
         }

@@ -7,11 +7,12 @@
 // (tmin, tend), ascending. A Gaussian is a candidate when its object-space ray hits the unit
 // instance box [-1,1]^3 within [tmin, tend] and passes the perpendicular-distance test.
 //
-// Pruning. Once the buffer is full, a subtree is skipped when its box entry exceeds
-// t_K + sqrt(3) kmax / |d|, where kmax bounds the kernel support of every Gaussian below it.
-// This is exact: for a candidate, |q(t)|^2 (q = object-space point) is a parabola in t with
-// curvature |d'|^2 >= |d|^2 / kmax^2 that is <= 3 somewhere inside the box, so
-// t* >= t_box_entry - sqrt(3) kmax / |d| >= t_node_entry - sqrt(3) kmax / |d|.
+// Culling follows the reference's traversal: subtrees are culled by their instance-box AABBs
+// against [tmin, t_K], where t_K is the K-th distance found so far (the reference's any-hit
+// program shrinks the ray's tmax to the 16th distance). This returns the K nearest candidates
+// except for a Gaussian whose closest approach lies before its own box entry (a ray grazing a
+// box corner, where the kernel response is below the acceptance threshold): like the
+// reference, it is then kept only if reached before t_K drops below its box entry.
 #pragma once
 
 #include "device_types.h"
@@ -25,7 +26,7 @@ constexpr unsigned kNoHit = 0xFFFFFFFFu;
 constexpr float kFarT = 1e20f;
 
 struct TraceCounters {
-    unsigned segments, calls, candidates, accepted, env, replay;
+    unsigned segments, calls, candidates, accepted, env, replay, replay_accepted, nodes, leaves;
 };
 
 PTIR_DEV void kbuf_clear(float (&kt)[kKBuf], unsigned (&kid)[kKBuf]) {
@@ -93,21 +94,23 @@ PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmi
 }
 
 // Fill (kt, kid) with the nearest candidates of ray (o, d) in (tmin, tend).
+// `stack` holds kStackDepth node indices, `stack_t` their entry distances.
 PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[kKBuf],
-                         unsigned (&kid)[kKBuf], int* stack, unsigned* err, TraceCounters& ctr) {
+                         unsigned (&kid)[kKBuf], int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
     kbuf_clear(kt, kid);
     ++ctr.calls;
     if (A.n <= 0) return;
     if (A.n == 1) {
+        ++ctr.leaves;
         test_leaf(A, 0, o, d, tmin, tend, kt, kid);
         ctr.candidates += kbuf_count(kid);
         return;
     }
     const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float margin = 1.7320508f * rsqrtf(dot(d, d));
     int sp = 0;
     int node = 0;
     while (true) {
+        ++ctr.nodes;
         const float4* nd = A.nodes + 4 * (size_t)node;
         const float4 a = __ldg(nd + 0), b = __ldg(nd + 1), c = __ldg(nd + 2), e = __ldg(nd + 3);
         const int left = __float_as_int(e.x), right = __float_as_int(e.y);
@@ -116,32 +119,49 @@ PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, flo
         slab(make_float3(b.z, b.w, c.x), make_float3(c.y, c.z, c.w), o, inv, r0, r1);
         l0 = fmaxf(l0, tmin);
         r0 = fmaxf(r0, tmin);
+        l1 = fminf(l1, tend);
+        r1 = fminf(r1, tend);
         const float cut = kt[kKBuf - 1];
-        bool hl = l0 <= fminf(l1, tend) && l0 <= cut + margin * e.z;
-        bool hr = r0 <= fminf(r1, tend) && r0 <= cut + margin * e.w;
+        bool hl = l0 <= l1 && l0 <= cut;
+        bool hr = r0 <= r1 && r0 <= cut;
         if (hl && left < 0) {
+            ++ctr.leaves;
             test_leaf(A, ~left, o, d, tmin, tend, kt, kid);
             hl = false;
         }
         if (hr && right < 0) {
+            ++ctr.leaves;
             test_leaf(A, ~right, o, d, tmin, tend, kt, kid);
             hr = false;
         }
         if (hl && hr) {
-            const bool lfirst = l0 <= r0;
+            // nearer middle of the clipped interval first: boxes that contain the origin all
+            // enter at tmin, their extent along the ray tells them apart
+            const bool lfirst = (l0 + l1) <= (r0 + r1);
             if (sp >= kStackDepth) {
                 atomicOr(err, kErrStackOverflow);
                 break;
             }
-            stack[sp++] = lfirst ? right : left;
+            stack[sp] = lfirst ? right : left;
+            stack_t[sp] = lfirst ? r0 : l0;
+            ++sp;
             node = lfirst ? left : right;
         } else if (hl) {
             node = left;
         } else if (hr) {
             node = right;
         } else {
-            if (sp == 0) break;
-            node = stack[--sp];
+            // pop the next subtree that can still hold a candidate nearer than the K-th
+            bool found = false;
+            while (sp > 0) {
+                --sp;
+                if (stack_t[sp] <= kt[kKBuf - 1]) {
+                    node = stack[sp];
+                    found = true;
+                    break;
+                }
+            }
+            if (!found) break;
         }
     }
     ctr.candidates += kbuf_count(kid);

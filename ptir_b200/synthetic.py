@@ -160,6 +160,34 @@ def view_rays(width: int, height: int, spp: int, eye, fov_deg: float = 40.0):
     return torch.from_numpy(np.stack(os_)), torch.from_numpy(np.stack(ds))
 
 
+def view_rays_device(width: int, height: int, spp: int, eye, device, fov_deg: float = 40.0):
+    """Same rays as view_rays(), computed with torch on `device` (float32): [spp, h, w, 3] x 2."""
+    pattern = SPP_PATTERNS.get(spp)
+    if pattern is None:
+        gw = int(math.ceil(math.sqrt(spp)))
+        gh = int(math.ceil(spp / gw))
+        pattern = tuple((((i % gw) + 0.5) / gw, ((i // gw) + 0.5) / gh) for i in range(spp))
+    eye = np.asarray(eye, np.float64)
+    fwd = -eye / np.linalg.norm(eye)
+    up = np.array([0.0, 0.0, 1.0])
+    if abs(np.dot(up, fwd)) > 0.999:
+        up = np.array([0.0, 1.0, 0.0])
+    right = np.cross(fwd, up)
+    right /= np.linalg.norm(right)
+    upv = np.cross(right, fwd)
+    th = math.tan(math.radians(fov_deg) * 0.5)
+    tw = th * width / height
+    f64 = dict(dtype=torch.float64, device=device)
+    jit = torch.tensor(pattern, **f64)  # [spp, 2]
+    xs = (torch.arange(width, **f64)[None, :] + jit[:, :1]) / width * 2.0 - 1.0  # [spp, w]
+    ys = 1.0 - (torch.arange(height, **f64)[None, :] + jit[:, 1:]) / height * 2.0  # [spp, h]
+    F, Rt, U = (torch.tensor(v, **f64) for v in (fwd, right, upv))
+    d = (F[None, None, None, :] + xs[:, None, :, None] * tw * Rt + ys[:, :, None, None] * th * U)
+    d = d / torch.linalg.norm(d, dim=-1, keepdim=True)
+    o = torch.tensor(eye, **f64).expand_as(d)
+    return o.float().contiguous(), d.float().contiguous()
+
+
 def density_tensor(f: dict) -> torch.Tensor:
     """[n,12] = pos, density, rot (wxyz), scale, 0 (threedgptir_tracer/tracer.py:163-165)."""
     return torch.cat([f["pos"], f["dns"], f["rot"], f["scl"], torch.zeros_like(f["dns"])], 1).contiguous()
