@@ -174,6 +174,24 @@ int ptir_debug_accel(ptir_tracer* tracer, float* nodes_host, float* leaves_host,
 
 const char* ptir_last_error(const ptir_tracer* tracer);
 
+/* Allocation-free scene bounds. This entry point has no counterpart in the reference.
+ * It is for callers that cannot allocate device memory once running, e.g. a process that
+ * reserves all device memory for its own pool at start-up, or a plugin whose host forbids
+ * device allocation after initialisation. For them a cudaMalloc fails or stalls the device.
+ * It writes the scene AABB of the Gaussians' instance boxes (the bounds every trace clips
+ * its rays to, identical to ptir_scene_bounds after ptir_build_bvh) into bounds_out:
+ * 8 floats, lo.xyz 0 hi.xyz 0, device memory, 16-byte aligned. Inputs are device pointers as in
+ * ptir_build_bvh, and kernel_degree / kernel_min_response / density_clamping are the
+ * ptir_config fields. No handle is needed and nothing is allocated: the only scratch is a
+ * fixed 128 KiB device array in the library.
+ * Limit: N <= 8,388,608; larger N returns PTIR_EINVAL. The first call on a device resolves the
+ * array's device address, so make that first call before any stream capture. Calls share the
+ * array: calls that overlap on the GPU (unordered streams) race. Errors are also described in
+ * err[err_len] when err is not NULL. */
+int ptir_instance_bounds_noalloc(float kernel_degree, float kernel_min_response, int32_t density_clamping,
+                                 const float* pos, const float* rot, const float* scl, const float* dns, int32_t n,
+                                 float* bounds_out, void* stream, char* err, int32_t err_len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -12,6 +12,12 @@
 // A refit (rebuild == false, same n) redoes 1, 2, 5 and 7 in the stored leaf order.
 #include <cub/device/device_radix_sort.cuh>
 
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/ptir_b200.h"
 #include "accel.h"
 #include "vecmath.cuh"
 
@@ -347,4 +353,129 @@ void accel_free(AccelState& st) {
     st = AccelState();
 }
 
+// ---------------------------------------------------------------------------------------
+// Allocation-free scene bounds (ptir_instance_bounds_noalloc).
+//
+// Some callers cannot allocate device memory once they are running. One example is a
+// renderer or serving process that reserves all device memory for its own pool at start-up.
+// Another is a plugin whose host forbids device allocation after initialisation. For them a
+// cudaMalloc either fails, or synchronises the whole device in the middle of a frame.
+// This entry point gives them the scene AABB of the Gaussians' instance boxes, the box every
+// trace clips its rays to, with no allocation at all. Its only scratch is the file-scope array
+// below.
+//
+// Limits. The array holds one partial AABB per block of kNoAllocItemsPerBlock Gaussians, for at
+// most kNoAllocMaxBlocks blocks: N <= 8,388,608 Gaussians, 128 KiB of scratch. Every GPU that
+// loads the library holds the array until the process exits. All calls share it. A call
+// writes the partial of every block it launches before reading it, so nothing needs clearing
+// between calls. Two calls that overlap on the GPU (unordered streams) race on it.
+namespace {
+
+constexpr int kNoAllocItemsPerBlock = 2048;
+constexpr int kNoAllocMaxBlocks = 4096;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) float4 g_noalloc_partial[2 * kNoAllocMaxBlocks];
+
+// the instance AABB of k_prep (8 transformed corners of [-1,1]^3), computed in place
+__device__ void instance_aabb(int g, const float* __restrict__ pos, const float* __restrict__ rot,
+                              const float* __restrict__ scl, const float* __restrict__ dns, const AccelBuildOptions& opt,
+                              float3& lo, float3& hi) {
+    const float4 q = make_float4(rot[4 * g], rot[4 * g + 1], rot[4 * g + 2], rot[4 * g + 3]);
+    const Mat3 R = quat_r(q);
+    const float ks = support_scale(dns[g], opt.min_response, opt.density_clamping, opt.kernel_degree);
+    const float3 k = make_float3(scl[3 * g], scl[3 * g + 1], scl[3 * g + 2]) * ks;
+    const float3 mu = make_float3(pos[3 * g], pos[3 * g + 1], pos[3 * g + 2]);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float3 corner = make_float3((c & 4) ? 1.0f : -1.0f, (c & 2) ? 1.0f : -1.0f, (c & 1) ? 1.0f : -1.0f);
+        const float3 v = mul_rows(R, corner * k) + mu;
+        lo = fmin3(lo, v);
+        hi = fmax3(hi, v);
+    }
+}
+
+// one partial AABB per block of kNoAllocItemsPerBlock consecutive Gaussians
+__global__ void k_bounds_noalloc_partial(int n, const float* __restrict__ pos, const float* __restrict__ rot,
+                                         const float* __restrict__ scl, const float* __restrict__ dns,
+                                         AccelBuildOptions opt, float4* __restrict__ partial) {
+    const int first = blockIdx.x * kNoAllocItemsPerBlock;
+    const int last = min(n, first + kNoAllocItemsPerBlock);
+    float3 lo = f3(3.0e38f), hi = f3(-3.0e38f);
+    for (int g = first + threadIdx.x; g < last; g += blockDim.x) instance_aabb(g, pos, rot, scl, dns, opt, lo, hi);
+    block_minmax(lo, hi);
+    if (threadIdx.x == 0) {
+        partial[2 * blockIdx.x] = make_float4(lo.x, lo.y, lo.z, 0.0f);
+        partial[2 * blockIdx.x + 1] = make_float4(hi.x, hi.y, hi.z, 0.0f);
+    }
+}
+
+std::mutex g_noalloc_mutex;
+float4* g_noalloc_device_ptr[kMaxDevices] = {};
+
+void set_error(char* buf, int len, const std::string& msg) {
+    if (!buf || len <= 0) return;
+    const size_t n = std::min<size_t>(msg.size(), (size_t)len - 1);
+    std::memcpy(buf, msg.data(), n);
+    buf[n] = '\0';
+}
+
+}  // namespace
+
 }  // namespace ptir
+
+extern "C" int ptir_instance_bounds_noalloc(float kernel_degree, float kernel_min_response, int32_t density_clamping,
+                                            const float* pos, const float* rot, const float* scl, const float* dns,
+                                            int32_t n, float* bounds_out, void* stream, char* err, int32_t err_len) {
+    using namespace ptir;
+    if (n < 0) {
+        set_error(err, err_len, "negative Gaussian count");
+        return PTIR_EINVAL;
+    }
+    if (n > kNoAllocItemsPerBlock * kNoAllocMaxBlocks) {
+        set_error(err, err_len, "n = " + std::to_string(n) + " exceeds the allocation-free limit of " +
+                                    std::to_string(kNoAllocItemsPerBlock * kNoAllocMaxBlocks) + " Gaussians");
+        return PTIR_EINVAL;
+    }
+    if (!bounds_out || (reinterpret_cast<uintptr_t>(bounds_out) & 15u) != 0) {
+        set_error(err, err_len, "bounds_out must be a 16-byte aligned device buffer of 8 floats");
+        return PTIR_EINVAL;
+    }
+    if (n > 0 && (!pos || !rot || !scl || !dns)) {
+        set_error(err, err_len, "null particle pointer");
+        return PTIR_EINVAL;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        set_error(err, err_len, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+        return PTIR_ECUDA;
+    }
+    float4* scratch = nullptr;
+    {
+        // set-up, once per device (with that device current): the array's device address
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_device_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_partial);
+            if (e != cudaSuccess) {
+                set_error(err, err_len, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+                return PTIR_ECUDA;
+            }
+            g_noalloc_device_ptr[dev] = static_cast<float4*>(p);
+        }
+        scratch = g_noalloc_device_ptr[dev];
+    }
+    const AccelBuildOptions opt{kernel_degree, kernel_min_response, density_clamping};
+    const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int blocks = (n + kNoAllocItemsPerBlock - 1) / kNoAllocItemsPerBlock;
+    if (blocks > 0) k_bounds_noalloc_partial<<<blocks, kReduceThreads, 0, s>>>(n, pos, rot, scl, dns, opt, scratch);
+    k_bounds_final<<<1, kReduceThreads, 0, s>>>(blocks, scratch, reinterpret_cast<float4*>(bounds_out));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error(err, err_len, std::string("launch: ") + cudaGetErrorString(e));
+        return PTIR_ECUDA;
+    }
+    set_error(err, err_len, "");
+    return PTIR_OK;
+}

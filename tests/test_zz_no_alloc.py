@@ -1,0 +1,63 @@
+"""The allocation-free scene-bounds entry point (ptir_instance_bounds_noalloc).
+
+It serves callers that cannot allocate device memory once running: a process that reserves
+all device memory for its own pool, or a plugin whose host forbids device allocation after
+start-up. The test calls it through the C ABI and checks its result against the existing
+path (ptir_build_bvh + ptir_scene_bounds) on two calls in a row. The second call covers fewer
+Gaussians than the first, so stale scratch from the first call must not leak into it. This
+file is collected last.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from ptir_b200 import _native
+from tests.scenes import make_tracer, small_scene
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-6, 1e-7
+
+
+def _bind():
+    lib = _native.load()
+    fn = lib.ptir_instance_bounds_noalloc
+    fn.argtypes = [C.c_float, C.c_float, C.c_int32] + [C.c_void_p] * 4 + [C.c_int32, C.c_void_p, C.c_void_p,
+                                                                          C.c_char_p, C.c_int32]
+    fn.restype = C.c_int
+    return fn
+
+
+def _noalloc_bounds(fn, S, n):
+    out = torch.full((8,), float("nan"), dtype=torch.float32, device="cuda")
+    err = C.create_string_buffer(256)
+    rc = fn(4.0, 0.0113, 1, S["build_pos"].data_ptr(), S["build_rot"].data_ptr(), S["build_scl"].data_ptr(),
+            S["build_dns"].data_ptr(), n, out.data_ptr(), torch.cuda.current_stream().cuda_stream, err, 256)
+    assert rc == 0, err.value
+    torch.cuda.synchronize()
+    o = out.cpu().numpy()
+    return np.concatenate([o[0:3], o[4:7]])
+
+
+def test_noalloc_bounds_match_build_bvh(cuda_device):
+    fn = _bind()
+    tr = make_tracer()
+    for n, seed in ((6000, 1), (1500, 2)):  # two calls in a row, the second one smaller
+        s = small_scene(n=n, w=8, h=8, seed=seed, layout="cluster_shell", scale_range=(0.002, 0.2))
+        S = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in s.items()
+             if k.startswith("build_")}
+        got = _noalloc_bounds(fn, S, n)
+        tr.build_bvh(S["build_pos"], S["build_rot"], S["build_scl"], S["build_dns"], True, True)
+        ref = tr.scene_bounds().numpy()
+        assert np.allclose(got, ref, rtol=RTOL, atol=ATOL), (n, got, ref)
+
+
+def test_noalloc_rejects_too_many_gaussians(cuda_device):
+    fn = _bind()
+    out = torch.empty((8,), dtype=torch.float32, device="cuda")
+    err = C.create_string_buffer(256)
+    rc = fn(4.0, 0.0113, 1, None, None, None, None, 8_388_609, out.data_ptr(), None, err, 256)
+    assert rc == _native.PTIR_EINVAL
+    assert b"exceeds the allocation-free limit" in err.value
