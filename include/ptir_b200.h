@@ -62,7 +62,14 @@ typedef struct ptir_config {
     int32_t enable_metallic;      /* render.enable_metallic */
     int32_t visualize_lights;     /* render.visualize_lights */
     int32_t collect_counters;     /* keep per-launch segment/candidate counters (cheap) */
+    /* B200 schedule (render.b200.*; no counterpart in the reference, results are identical): */
+    int32_t schedule;             /* PTIR_SCHEDULE_WAVEFRONT (default) or PTIR_SCHEDULE_MEGAKERNEL */
+    int32_t chunk_tiles;          /* wavefront: 8x4 pixel tiles per chunk of paths (0 = default 131072) */
+    int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16). The
+                                     hits are composited in the same order for every size. */
 } ptir_config;
+
+enum { PTIR_SCHEDULE_WAVEFRONT = 0, PTIR_SCHEDULE_MEGAKERNEL = 1 };
 
 /* Inputs of one trace, shared by the forward and the backward
  * (the arguments of OptixTracer::trace, optixTracer.h:148-168). */

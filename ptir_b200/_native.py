@@ -32,7 +32,13 @@ class PtirConfig(C.Structure):
         ("enable_metallic", C.c_int32),
         ("visualize_lights", C.c_int32),
         ("collect_counters", C.c_int32),
+        ("schedule", C.c_int32),
+        ("chunk_tiles", C.c_int32),
+        ("kbuffer", C.c_int32),
     ]
+
+
+SCHEDULES = {"wavefront": 0, "megakernel": 1}
 
 
 class PtirTraceArgs(C.Structure):

@@ -7,10 +7,12 @@
 #include "../../include/ptir_b200.h"
 #include "accel.h"
 #include "device_types.h"
+#include "wavefront.h"
 
 struct ptir_tracer {
     ptir_config cfg;
     ptir::AccelState accel;
+    ptir::WavefrontBuffers wave;
     unsigned* error_word = nullptr;
     unsigned long long* counters = nullptr;
     std::string last_error;
@@ -28,6 +30,8 @@ int cuda_fail(ptir_tracer* t, cudaError_t e, const char* what) {
 }
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+unsigned chunk_tiles_of(const ptir_config& c) { return c.chunk_tiles > 0 ? (unsigned)c.chunk_tiles : 131072u; }
 
 unsigned flags_of(const ptir_config& c) {
     unsigned f = 0;
@@ -47,6 +51,7 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, ptir::TraceParams& p) {
     if (launches > 0 && (!a->ray_origin || !a->ray_direction || !a->ray_to_world))
         return fail(t, PTIR_EINVAL, "ray_origin, ray_direction and ray_to_world are required");
     if (launches > (1ll << 31) - 1) return fail(t, PTIR_EINVAL, "launch extent exceeds 2^31 - 1 paths");
+    if (a->max_bounces > 64) return fail(t, PTIR_EINVAL, "max_bounces above 64");
     if (!t->accel.valid) return fail(t, PTIR_ESTATE, "trace called before build_bvh");
     if (a->n != t->accel.n)
         return fail(t, PTIR_ESTATE, "particle count " + std::to_string(a->n) + " differs from the acceleration structure (" +
@@ -125,6 +130,9 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     const int ideg = (int)deg;
     if (!(ideg == 0 || ideg == 1 || ideg == 2 || ideg == 3 || ideg == 4 || ideg == 5 || ideg == 8)) return PTIR_EINVAL;
     if (!(config->kernel_min_response > 0.0f && config->kernel_min_response < 1.0f)) return PTIR_EINVAL;
+    if (config->schedule != PTIR_SCHEDULE_WAVEFRONT && config->schedule != PTIR_SCHEDULE_MEGAKERNEL) return PTIR_EINVAL;
+    if (config->chunk_tiles < 0) return PTIR_EINVAL;
+    if (!(config->kbuffer == 0 || config->kbuffer == 8 || config->kbuffer == 16 || config->kbuffer == 32)) return PTIR_EINVAL;
     ptir_tracer* t = new ptir_tracer();
     t->cfg = *config;
     if (cudaMalloc(&t->error_word, sizeof(unsigned)) != cudaSuccess ||
@@ -144,6 +152,7 @@ void ptir_destroy(ptir_tracer* t) {
     if (!t) return;
     cudaDeviceSynchronize();
     ptir::accel_free(t->accel);
+    ptir::wavefront_free(t->wave);
     cudaFree(t->error_word);
     cudaFree(t->counters);
     delete t;
@@ -198,7 +207,9 @@ int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_output
     fo.light = o->light;
     fo.components = o->pbr_components;
     fo.visibility = o->visibility;
-    e = ptir::launch_trace_fwd(p, fo, 128, s);
+    e = t->cfg.schedule == PTIR_SCHEDULE_MEGAKERNEL
+            ? ptir::launch_trace_fwd(p, fo, 128, s)
+            : ptir::launch_trace_fwd_wavefront(p, fo, t->wave, chunk_tiles_of(t->cfg), t->cfg.kbuffer, s);
     if (e != cudaSuccess) return cuda_fail(t, e, "trace launch");
     return PTIR_OK;
 }
@@ -236,7 +247,9 @@ int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args
     bi.material_grad = b->material_grad;
     bi.particle_material_grad = o->particle_material_grad;
     bi.environment_grad = env ? o->environment_grad : nullptr;
-    e = ptir::launch_trace_bwd(p, bi, 128, s);
+    e = t->cfg.schedule == PTIR_SCHEDULE_MEGAKERNEL
+            ? ptir::launch_trace_bwd(p, bi, 128, s)
+            : ptir::launch_trace_bwd_wavefront(p, bi, t->wave, chunk_tiles_of(t->cfg), t->cfg.kbuffer, s);
     if (e != cudaSuccess) return cuda_fail(t, e, "trace_bwd launch");
     return PTIR_OK;
 }

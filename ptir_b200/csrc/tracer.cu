@@ -4,359 +4,17 @@
 // reference raygen programs do (threedgptir_tracer/src/kernels/cuda/referenceOptix.cu:27-71,
 // referenceBwdOptix.cu:27-74). Each warp covers an 8x4 pixel tile so primary rays of a warp
 // are coherent. Candidate gathering is the software LBVH traversal of traverse.cuh.
-#include "device_types.h"
-#include "pcg.cuh"
-#include "shading.cuh"
-#include "traverse.cuh"
-#include "vecmath.cuh"
+#include "path.cuh"
 
 namespace ptir {
 
 // ------------------------------------------------------------------------------------
-// per-segment state (the reference's rayPayload, threedgptir_tracer/include/3dgptir/payLoad.h:38-95)
-struct Segment {
-    float3 o, d;
-    float3 radiance, normal, light, ray_dir_grad;
-    float transmittance, depth, hit2, last_hit, distortion, hits_count;
-    float scatter_pdf, light_pdf;
-    bool hit, escaped;
-    // interaction (interaction.h:22-76)
-    bool ivalid;
-    float3 pos, snrm, albedo;
-    float rough, metal;
-    float3 d_albedo;
-    float d_rough, d_metal;
-};
-
-PTIR_DEV void segment_reset(Segment& s, float3 o, float3 d, float last_hit) {
-    s.o = o;
-    s.d = d;
-    s.radiance = s.normal = s.light = s.ray_dir_grad = f3(0.0f);
-    s.transmittance = 1.0f;
-    s.depth = s.hit2 = s.distortion = s.hits_count = 0.0f;
-    s.last_hit = last_hit;
-    s.scatter_pdf = s.light_pdf = 0.0f;
-    s.hit = s.escaped = false;
-    s.ivalid = false;
-    s.pos = s.snrm = s.albedo = f3(0.0f);
-    s.rough = s.metal = 0.0f;
-    s.d_albedo = f3(0.0f);
-    s.d_rough = s.d_metal = 0.0f;
-}
-
-struct Emitter {
-    float3 dir, contribution;
-    float light_pdf, scatter_pdf;
-};
-
-struct PathState {
-    unsigned active, bounces, max_bounces;
-    float3 acc, acc_grad, acc_direct, acc_indirect, acc_light, acc_light_grad, throughput;
-    Emitter em;
-    // pending roughness gradient through the next direction (payLoad.h:97-138)
-    bool pend_valid;
-    float3 pend_o, pend_d, pend_dnext;
-    float pend_opacity, pend_max_hit;
-    unsigned pend_bounces;
-};
-
-struct Ctx {
-    const TraceParams& P;
-    int* stack;
-    float* stack_t;
-    TraceCounters& ctr;
-};
-
-// scene AABB interval, clamped at 0 (pathTracer.cuh:46-52)
-PTIR_DEV float2 clip_scene(const TraceParams& P, float3 o, float3 d) {
-    if (P.accel.n <= 0) return make_float2(1.0f, 0.0f);
-    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    const float4 lo = __ldg(P.accel.bounds), hi = __ldg(P.accel.bounds + 1);
-    float t0, t1;
-    slab(make_float3(lo.x, lo.y, lo.z), make_float3(hi.x, hi.y, hi.z), o, inv, t0, t1);
-    return make_float2(fmaxf(0.0f, t0), t1);
-}
-
-// shared front of the hit evaluation: the particle frame, squared distance and response
-struct Response {
-    float3 gro, grd, scl;
-    Mat3 rt;
-    float d2, gres, alpha;
-};
-
-PTIR_DEV float kernel_response(int degree, float d2) {
-    switch (degree) {
-    case 8: { const float q = d2 * d2; return __expf(-0.000685871056241f * q * q); }
-    case 5: return __expf(-0.0185185185185f * d2 * d2 * sqrtf(d2));
-    case 4: return __expf(-0.0555555555556f * d2 * d2);
-    case 3: return __expf(-0.166666666667f * d2 * sqrtf(d2));
-    case 1: return __expf(-1.5f * sqrtf(d2));
-    case 0: return fmaxf(1.0f - 0.329630334487f * sqrtf(d2), 0.0f);
-    default: return __expf(-0.5f * d2);
-    }
-}
-
-PTIR_DEV Response respond(const TraceParams& P, unsigned id, float3 o, float3 d, float& density) {
-    const float4* rec = P.part.density + 3 * (size_t)id;
-    const float4 a = __ldg(rec + 0), q = __ldg(rec + 1), c = __ldg(rec + 2);
-    Response r;
-    r.rt = quat_rt(q);
-    r.scl = make_float3(c.x, c.y, c.z);
-    const float3 is = make_float3(1.0f / c.x, 1.0f / c.y, 1.0f / c.z);
-    r.gro = is * mul_rows(r.rt, o - make_float3(a.x, a.y, a.z));
-    r.grd = normalize_or_keep(is * mul_rows(r.rt, d));
-    const float3 cr = cross(r.grd, r.gro);
-    r.d2 = dot(cr, cr);
-    r.gres = kernel_response(P.kernel_degree, r.d2);
-    density = a.w;
-    r.alpha = fminf(0.99f, r.gres * a.w);
-    return r;
-}
-
-// secondary rays skip Gaussians just in front of the origin whose shading normal faces along
-// the ray (pathTracer.cuh:115-128)
-PTIR_DEV bool self_occluded(const TraceParams& P, float t, unsigned id, float3 d) {
-    if (t > (1e-1f - 2e-2f) || P.part.snrm == nullptr) return false;
-    return dot(ld3(P.part.snrm + 3 * (size_t)id), d) > 0.1f;
-}
-
-// SH radiance of degree <= 3 (+0.5 bias, clamped at 0) along direction d
-PTIR_DEV float3 sh_radiance(const TraceParams& P, unsigned id, float3 d) {
-    const float* c = P.part.sph + (size_t)id * P.part.sph_stride;
-    float3 rad = ld3(c) * 0.28209479177387814f;
-    const int deg = P.part.sph_degree;
-    if (deg > 0) {
-        const float x = d.x, y = d.y, z = d.z;
-        rad = rad - ld3(c + 3) * (0.4886025119029199f * y) + ld3(c + 6) * (0.4886025119029199f * z) -
-              ld3(c + 9) * (0.4886025119029199f * x);
-        if (deg > 1) {
-            const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-            rad = rad + ld3(c + 12) * (1.0925484305920792f * xy) + ld3(c + 15) * (-1.0925484305920792f * yz) +
-                  ld3(c + 18) * (0.31539156525252005f * (2.0f * zz - xx - yy)) +
-                  ld3(c + 21) * (-1.0925484305920792f * xz) + ld3(c + 24) * (0.5462742152960396f * (xx - yy));
-            if (deg > 2) {
-                rad = rad + ld3(c + 27) * (-0.5900435899266435f * y * (3.0f * xx - yy)) +
-                      ld3(c + 30) * (2.890611442640554f * xy * z) +
-                      ld3(c + 33) * (-0.4570457994644658f * y * (4.0f * zz - xx - yy)) +
-                      ld3(c + 36) * (0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy)) +
-                      ld3(c + 39) * (-0.4570457994644658f * x * (4.0f * zz - xx - yy)) +
-                      ld3(c + 42) * (1.445305721320277f * z * (xx - yy)) +
-                      ld3(c + 45) * (-0.5900435899266435f * x * (xx - 3.0f * yy));
-            }
-        }
-    }
-    return relu3(rad + f3(0.5f));
-}
-
-// Stochastic shadow transmittance: occluded at the first hit whose alpha beats a draw
-// (pathTracer.cuh:130-214).
-PTIR_DEV bool shadow_occluded(const Ctx& C, float3 o, float3 d, Pcg32& rng) {
-    const TraceParams& P = C.P;
-    const float2 clip = clip_scene(P, o, d);
-    float start = fmaxf(0.0f, clip.x - 1e-9f);
-    const float end = fminf(kFarT, clip.y) + 1e-9f;
-    if (start >= end) return false;
-    float kt[kKBuf];
-    unsigned kid[kKBuf];
-    for (int round = 0; start < end; ++round) {
-        if (round > (1 << 16)) {
-            atomicOr(P.error_word, kErrLoopBound);
-            break;
-        }
-        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
-        if (kid[0] == kNoHit) break;
-        float batch_end = start;
-        bool stop = false;
-#pragma unroll
-        for (int i = 0; i < kKBuf; ++i) {
-            if (stop) continue;
-            const unsigned id = kid[i];
-            if (id == kNoHit || kt[i] > end) { stop = true; continue; }
-            batch_end = fmaxf(batch_end, kt[i]);
-            if (self_occluded(P, kt[i], id, d)) continue;
-            float dns;
-            const Response r = respond(P, id, o, d, dns);
-            const float alpha = (r.gres > P.min_response && r.alpha > P.alpha_min) ? r.alpha : 0.0f;
-            if (alpha > 0.0f && rng.uniform() < alpha) return true;
-        }
-        if (batch_end <= start) break;
-        start = batch_end;
-    }
-    return false;
-}
-
-PTIR_DEV void shading_frame(const Segment& s, float3& n, float3& wo, float3& alb, float& met, bool metallic_on) {
-    n = normalize_or(s.snrm, make_float3(0.0f, 0.0f, 1.0f));
-    wo = normalize_or(-s.d, n);
-    alb = saturate(s.albedo);
-    met = metallic_on ? saturate(s.metal) : 0.0f;
-}
-
-// Next-event estimation toward the environment (pathTracer.cuh:461-504)
-PTIR_DEV void sample_nee(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
-    const TraceParams& P = C.P;
-    ps.em.contribution = f3(0.0f);
-    ps.em.light_pdf = 0.0f;
-    ps.em.scatter_pdf = 0.0f;
-    ps.em.dir = f3(0.0f);
-    float lpdf = 0.0f;
-    float3 wi = f3(0.0f), Li = f3(0.0f);
-    if (env_light_present(P.env)) {
-        wi = sample_env_direction(P.env, rng, lpdf);
-        Li = env_radiance(P.env, wi, C.ctr.env);
-    }
-    if (lpdf <= 0.0f || all_zero(Li)) return;
-    if (dot(s.snrm, wi) <= 0.0f) return;
-    float3 n, wo, alb;
-    float met;
-    const bool metallic_on = (P.flags & kMetallic) != 0;
-    shading_frame(s, n, wo, alb, met, metallic_on);
-    float spdf;
-    const BrdfTerms bc = eval_brdf<false>(wo, n, alb, met, clamp_rough(s.rough), wi, metallic_on, spdf);
-    ++C.ctr.segments;
-    if (shadow_occluded(C, s.pos + wi * 2e-2f, wi, rng)) return;
-    ps.em.dir = wi;
-    ps.em.light_pdf = lpdf;
-    ps.em.scatter_pdf = spdf;
-    ps.em.contribution = ps.throughput * bc.value * Li / fmaxf(lpdf, 1e-6f);
-}
-
-// BRDF-sampled continuation (pathTracer.cuh:430-459)
-PTIR_DEV void sample_next(const Ctx& C, PathState& ps, Segment& s, Pcg32& rng) {
-    const TraceParams& P = C.P;
-    float3 n, wo, alb;
-    float met;
-    const bool metallic_on = (P.flags & kMetallic) != 0;
-    shading_frame(s, n, wo, alb, met, metallic_on);
-    float3 next = s.d;
-    const float3 rnd = rng.uniform3();
-    const BrdfSample b = sample_brdf<false>(wo, n, alb, met, clamp_rough(s.rough), rnd, metallic_on, next);
-    const float3 nt = ps.throughput * b.value;
-    if (all_zero(nt)) {
-        ps.throughput = f3(0.0f);
-        ps.active = 0u;
-        return;
-    }
-    ps.throughput = nt;
-    const float3 origin = s.pos + normalize_or_keep(next) * 2e-2f;
-    segment_reset(s, origin, next, 0.0f);
-    if (P.flags & kMis) {
-        s.scatter_pdf = b.pdf;
-        s.light_pdf = env_pdf(P.env, next);
-    }
-}
-
-// Radiance gathered at the end of a segment (environment.cuh:636-715)
-PTIR_DEV void accumulate_light(const Ctx& C, PathState& ps, Segment& s) {
-    const TraceParams& P = C.P;
-    const bool first = ps.bounces == 1u;
-    const bool mis = (P.flags & kMis) != 0;
-    float bmis = 1.0f, lmis = 1.0f;
-    if (mis && first) {
-        bmis = mis_weight(s.scatter_pdf, s.light_pdf);
-        lmis = mis_weight(ps.em.light_pdf, ps.em.scatter_pdf);
-    }
-    const float3 nee = ps.em.contribution * lmis;
-    if (P.render_opts == 1u) {
-        if (mis && first) ps.acc += nee;
-        if (ps.bounces > 0u && s.ivalid) {
-            float3 contrib = ps.throughput * s.radiance;
-            if (mis && first) contrib *= bmis;
-            ps.acc += contrib;
-            ps.acc_indirect += contrib;
-        } else if (s.escaped) {
-            if (!env_present(P.env)) return;
-            const float3 vr = env_radiance(P.env, s.d, C.ctr.env);
-            ps.throughput *= s.transmittance;
-            s.light += vr;
-            ps.acc_light += vr;
-            float3 contrib = ps.throughput * s.light;
-            if (mis && first) contrib *= bmis;
-            ps.acc += contrib;
-            ps.acc_direct += contrib;
-        }
-        return;
-    }
-    if (mis && first) {
-        ps.acc += nee;
-        ps.acc_direct += nee;
-    }
-    if (s.escaped) {
-        if (!env_present(P.env)) return;
-        const float3 vr = env_radiance(P.env, s.d, C.ctr.env);
-        ps.throughput *= s.transmittance;
-        s.light += vr;
-        ps.acc_light += vr;
-        float3 contrib = ps.throughput * s.light;
-        if (mis && first) contrib *= bmis;
-        s.radiance += contrib;
-        ps.acc += contrib;
-        if (ps.bounces < 2u) ps.acc_direct += contrib;
-        else ps.acc_indirect += contrib;
-    }
-}
-
-PTIR_DEV void path_init(PathState& ps, unsigned max_bounces) {
-    ps.active = 1u;
-    ps.bounces = 0u;
-    ps.max_bounces = max_bounces;
-    ps.acc = ps.acc_grad = ps.acc_direct = ps.acc_indirect = ps.acc_light = ps.acc_light_grad = f3(0.0f);
-    ps.throughput = f3(1.0f);
-    ps.em.dir = ps.em.contribution = f3(0.0f);
-    ps.em.light_pdf = ps.em.scatter_pdf = 0.0f;
-    ps.pend_valid = false;
-    ps.pend_o = ps.pend_d = ps.pend_dnext = f3(0.0f);
-    ps.pend_opacity = ps.pend_max_hit = 0.0f;
-    ps.pend_bounces = 0u;
-}
-
-PTIR_DEV void world_ray(const TraceParams& P, size_t li, float3& o, float3& d) {
-    const float* m = P.ray_to_world;
-    const float3 lo = ld3(P.ray_ori + 3 * li), ld = ld3(P.ray_dir + 3 * li);
-    const float3 m0 = ld3(m), m1 = ld3(m + 4), m2 = ld3(m + 8);
-    o = make_float3(dot(m0, lo) + __ldg(m + 3), dot(m1, lo) + __ldg(m + 7), dot(m2, lo) + __ldg(m + 11));
-    d = make_float3(dot(m0, ld), dot(m1, ld), dot(m2, ld));
-}
-
-PTIR_DEV unsigned effective_bounces(const TraceParams& P) {
-    return P.render_opts ? min(P.max_bounces, 2u) : P.max_bounces;
-}
-
-// launch index of this thread: warps own 8x4 pixel tiles, tiles row-major, then z
-PTIR_DEV bool launch_index(const TraceParams& P, unsigned& x, unsigned& y, unsigned& z) {
-    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned tiles_x = (unsigned)(P.w + 7) >> 3, tiles_y = (unsigned)(P.h + 3) >> 2;
-    const unsigned per_z = tiles_x * tiles_y;
-    z = warp / per_z;
-    const unsigned t = warp - z * per_z;
-    const unsigned ty = t / tiles_x, tx = t - ty * tiles_x;
-    x = (tx << 3) + (lane & 7u);
-    y = (ty << 2) + (lane >> 3);
-    return z < (unsigned)P.nz && x < (unsigned)P.w && y < (unsigned)P.h;
-}
-
-PTIR_DEV void flush_counters(const TraceParams& P, const TraceCounters& c) {
-    if (P.counters == nullptr) return;
-    const unsigned v[9] = {c.segments, c.calls, c.candidates, c.accepted, c.env, c.replay, c.replay_accepted, c.nodes,
-                           c.leaves};
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-        const unsigned s = __reduce_add_sync(0xFFFFFFFFu, v[k]);
-        if ((threadIdx.x & 31u) == 0u && s) atomicAdd(P.counters + k, (unsigned long long)s);
-    }
-}
-
-// ------------------------------------------------------------------------------------
 // forward (referenceOptix.cu:27-71)
-template <bool kSelfOcc>
-PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis);
-
 __global__ void __launch_bounds__(128) k_trace_fwd(TraceParams P, FwdOutputs O) {
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    Ctx C{P, stack, stack_t, ctr};
+    CtxT<kKBuf> C{P, stack, stack_t, ctr};
     unsigned x, y, z;
     if (launch_index(P, x, y, z)) {
         const size_t li = ((size_t)z * P.h + y) * P.w + x;
@@ -413,296 +71,13 @@ __global__ void __launch_bounds__(128) k_trace_fwd(TraceParams P, FwdOutputs O) 
     flush_counters(P, ctr);
 }
 
-// Front-to-back compositing of one segment over k-buffer batches (pathTracer.cuh:216-311 with
-// processHit, gaussianParticles.cuh:343-440). Accepted Gaussians are flagged in `vis` (when
-// given) as int32 1 inside the float32 tensor, as the reference does (pathTracer.cuh:283-284).
-template <bool kSelfOcc>
-PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
-    const TraceParams& P = C.P;
-    const float2 clip = clip_scene(P, s.o, s.d);
-    const float keep_spdf = s.scatter_pdf, keep_lpdf = s.light_pdf;
-    segment_reset(s, s.o, s.d, fmaxf(0.0f, clip.x - 1e-9f));
-    if (P.flags & kMis) {
-        s.scatter_pdf = keep_spdf;
-        s.light_pdf = keep_lpdf;
-    }
-    const bool normals = (P.flags & kNormals) != 0;
-    float3 m_alb = f3(0.0f), snrm = f3(0.0f);
-    float m_rgh = 0.0f, m_met = 0.0f;
-    float kt[kKBuf];
-    unsigned kid[kKBuf];
-    for (int round = 0; s.last_hit <= clip.y && s.transmittance > P.min_transmittance; ++round) {
-        if (round > (1 << 16)) {
-            atomicOr(P.error_word, kErrLoopBound);
-            break;
-        }
-        trace_kbuf(P.accel, s.o, s.d, s.last_hit + 1e-9f, clip.y + 1e-9f, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
-        if (kid[0] == kNoHit) break;
-#pragma unroll
-        for (int i = 0; i < kKBuf; ++i) {
-            const unsigned id = kid[i];
-            if (id == kNoHit || !(s.transmittance > P.min_transmittance)) continue;
-            if (kSelfOcc && self_occluded(P, kt[i], id, s.d)) {
-                s.last_hit = fmaxf(s.last_hit, kt[i]);
-                continue;
-            }
-            float dns;
-            const Response r = respond(P, id, s.o, s.d, dns);
-            const bool accept = r.gres > P.min_response && r.alpha > P.alpha_min;
-            if (accept) {
-                ++C.ctr.accepted;
-                const float w = r.alpha * s.transmittance;
-                const float3 grds = r.scl * r.grd * dot(r.grd, -r.gro);
-                const float hit_t = sqrtf(dot(grds, grds));
-                s.radiance += sh_radiance(P, id, s.d) * w;
-                const float* m = P.part.material + 5 * (size_t)id;
-                m_alb += ld3(m) * w;
-                m_rgh += __ldg(m + 3) * w;
-                m_met += __ldg(m + 4) * w;
-                s.transmittance *= (1.0f - r.alpha);
-                s.depth += hit_t * w;
-                s.hit2 += hit_t * hit_t * w;
-                if (normals) {
-                    snrm += ld3(P.part.snrm + 3 * (size_t)id) * w;
-                    const float3 srot = mul_cols(r.rt, r.scl);
-                    s.normal += normalize_or_keep((r.gro + r.grd * (dot(r.grd, -r.gro) - sqrtf(9.0f - r.d2))) * srot) * w;
-                }
-                s.hit = true;
-                const float op = 1.0f - s.transmittance;
-                s.distortion = fmaxf(op * s.hit2 - s.depth * s.depth, 0.0f);
-                if (vis) vis[id] = __int_as_float(1);
-            }
-            s.last_hit = fmaxf(s.last_hit, kt[i]);
-            if (P.flags & kHitCounts) s.hits_count += accept ? 1.0f : 0.0f;
-        }
-    }
-    const float op = 1.0f - s.transmittance;
-    if (s.hit && op > 0.5f) {
-        const float inv = 1.0f / fmaxf(op, 1e-12f);
-        s.ivalid = true;
-        s.pos = s.o + s.d * (s.depth * inv);
-        s.snrm = snrm * inv;
-        s.albedo = m_alb * inv;
-        s.rough = m_rgh * inv;
-        s.metal = m_met * inv;
-    } else {
-        s.escaped = rng.uniform() < s.transmittance;
-    }
-}
-
 // ------------------------------------------------------------------------------------
-// backward: path replay ("radiative backprop") of referenceBwdOptix.cu:27-74
-
-// material gradient of the Gaussians composited along a segment (pathTracer.cuh:313-390)
-PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, bool self_occ, float3 o, float3 d, float opacity,
-                                   float max_hit, float3 da, float dr, float dm) {
-    const TraceParams& P = C.P;
-    ++C.ctr.replay;
-    const float inv = 1.0f / fmaxf(opacity, 1e-12f);
-    da = da * inv;
-    dr *= inv;
-    dm *= inv;
-    const bool metallic_on = (P.flags & kMetallic) != 0;
-    const float2 clip = clip_scene(P, o, d);
-    float start = fmaxf(0.0f, clip.x - 1e-9f);
-    const float end = fminf(max_hit, clip.y) + 1e-9f;
-    float tr = 1.0f;
-    float kt[kKBuf];
-    unsigned kid[kKBuf];
-    for (int round = 0; start < end && tr > P.min_transmittance; ++round) {
-        if (round > (1 << 16)) {
-            atomicOr(P.error_word, kErrLoopBound);
-            break;
-        }
-        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
-        if (kid[0] == kNoHit) break;
-#pragma unroll
-        for (int i = 0; i < kKBuf; ++i) {
-            const unsigned id = kid[i];
-            if (id == kNoHit || !(tr > P.min_transmittance)) continue;
-            if (self_occ && self_occluded(P, kt[i], id, d)) {
-                start = fmaxf(start, kt[i]);
-                continue;
-            }
-            float dns;
-            const Response r = respond(P, id, o, d, dns);
-            if (r.gres > P.min_response && r.alpha > P.alpha_min) {
-                ++C.ctr.replay_accepted;
-                const float w = r.alpha * tr;
-                float* g = B.particle_material_grad + 5 * (size_t)id;
-                atomicAdd(g + 0, w * da.x);
-                atomicAdd(g + 1, w * da.y);
-                atomicAdd(g + 2, w * da.z);
-                atomicAdd(g + 3, w * dr);
-                if (metallic_on) atomicAdd(g + 4, w * dm);
-                tr *= (1.0f - r.alpha);
-            }
-            start = fmaxf(start, kt[i]);
-        }
-    }
-}
-
-// environment texel gradient of a bilinear lookup plus the finite-difference direction gradient
-// (environment.cuh:89-114, 421-473)
-PTIR_DEV float3 env_radiance_bwd(const Ctx& C, const BwdInputs& B, float3 d, float3 cg, float3& dir_grad) {
-    const EnvView& E = C.P.env;
-    if (!env_present(E)) return f3(0.0f);
-    const Footprint f = footprint_of(E, env_rotate(E, d));
-    const float3 bg = bilerp(E, f);
-    ++C.ctr.env;
-    if (B.environment_grad) {
-        auto add = [&](int x, int y, float w) {
-            float* g = B.environment_grad + 4 * ((size_t)y * E.w + x);
-            atomicAdd(g + 0, w * cg.x);
-            atomicAdd(g + 1, w * cg.y);
-            atomicAdd(g + 2, w * cg.z);
-        };
-        add(f.x0, f.y0, f.w00);
-        add(f.x1, f.y0, f.w10);
-        add(f.x0, f.y1, f.w01);
-        add(f.x1, f.y1, f.w11);
-    }
-    const float3 u = normalize_or_keep(d);
-    float3 t, b;
-    onb(u, t, b);
-    const float eps = 1e-3f;
-    const float ps = rsqrtf(1.0f + eps * eps);
-    const float3 tb = bilerp(E, footprint_of(E, env_rotate(E, (u + t * eps) * ps)));
-    const float3 bb = bilerp(E, footprint_of(E, env_rotate(E, (u + b * eps) * ps)));
-    C.ctr.env += 2;
-    const float ie = 1.0f / eps;
-    dir_grad += t * dot((tb - bg) * ie, cg) + b * dot((bb - bg) * ie, cg);
-    return bg;
-}
-
-// environment.cuh:717-808
-PTIR_DEV void accumulate_light_bwd(const Ctx& C, const BwdInputs& B, PathState& ps, Segment& s) {
-    const TraceParams& P = C.P;
-    const bool first = ps.bounces == 1u;
-    const bool mis = (P.flags & kMis) != 0;
-    float bmis = 1.0f, lmis = 1.0f;
-    if (mis && first) {
-        bmis = mis_weight(s.scatter_pdf, s.light_pdf);
-        lmis = mis_weight(ps.em.light_pdf, ps.em.scatter_pdf);
-    }
-    if (P.render_opts == 1u) {
-        if (mis && first) ps.acc -= ps.em.contribution * lmis;
-        if (ps.bounces > 0u && s.ivalid) {
-            float3 contrib = ps.throughput * s.radiance;
-            if (mis && first) contrib *= bmis;
-            ps.acc -= contrib;
-        } else if (s.escaped) {
-            if (!env_present(P.env)) return;
-            ps.throughput *= s.transmittance;
-            float3 eg = ps.acc_grad * ps.throughput;
-            if (mis && first) eg *= bmis;
-            eg += ps.acc_light_grad;
-            const float3 vr = env_radiance_bwd(C, B, s.d, eg, s.ray_dir_grad);
-            float3 contrib = ps.throughput * vr;
-            if (mis && first) contrib *= bmis;
-            ps.acc -= contrib;
-        }
-        return;
-    }
-    if (mis && first) ps.acc -= ps.em.contribution * lmis;
-    if (s.escaped) {
-        if (!env_present(P.env)) return;
-        ps.throughput *= s.transmittance;
-        float3 eg = ps.acc_grad * ps.throughput;
-        if (mis && first) eg *= bmis;
-        eg += ps.acc_light_grad;
-        const float3 vr = env_radiance_bwd(C, B, s.d, eg, s.ray_dir_grad);
-        float3 contrib = ps.throughput * vr;
-        if (mis && first) contrib *= bmis;
-        s.radiance += contrib;
-        ps.acc -= contrib;
-    }
-}
-
-// pathTracer.cuh:392-428
-PTIR_DEV void pending_bwd(const Ctx& C, const BwdInputs& B, PathState& ps, const Segment& s) {
-    if (!ps.pend_valid) return;
-    const float dr = dot(s.ray_dir_grad, ps.pend_dnext);
-    ps.pend_valid = false;
-    if (dr == 0.0f) return;
-    replay_material_grad(C, B, ps.pend_bounces > 1u, ps.pend_o, ps.pend_d, ps.pend_opacity, ps.pend_max_hit, f3(0.0f), dr,
-                         0.0f);
-}
-
-// pathTracer.cuh:506-548 (albedo only; the environment and roughness terms are disabled there)
-PTIR_DEV void nee_grad_bwd(const Ctx& C, PathState& ps, Segment& s, const Segment& it) {
-    const TraceParams& P = C.P;
-    if (ps.bounces != 1u || ps.em.light_pdf <= 0.0f) return;
-    float3 n, wo, alb;
-    float met;
-    const bool metallic_on = (P.flags & kMetallic) != 0;
-    shading_frame(it, n, wo, alb, met, metallic_on);
-    float spdf;
-    const BrdfTerms g = eval_brdf<true>(wo, n, alb, met, it.rough, ps.em.dir, metallic_on, spdf);
-    const float scale = mis_weight(ps.em.light_pdf, ps.em.scatter_pdf) / fmaxf(ps.em.light_pdf, 1e-6f);
-    const float3 bgc = env_radiance(P.env, ps.em.dir, C.ctr.env);
-    const float3 dl = ps.acc_grad * ps.throughput * bgc * scale;
-    s.d_albedo += dl * g.d_albedo;
-}
-
-// pathTracer.cuh:551-634
-PTIR_DEV void sample_next_bwd(const Ctx& C, const BwdInputs& B, PathState& ps, Segment& s, Pcg32& rng) {
-    const TraceParams& P = C.P;
-    const bool metallic_on = (P.flags & kMetallic) != 0;
-    const bool mis = (P.flags & kMis) != 0;
-    const Segment it = s;  // the interaction being scattered from
-    float3 n, wo, alb;
-    float met;
-    shading_frame(it, n, wo, alb, met, metallic_on);
-    float3 next = it.d;
-    const float3 rnd = rng.uniform3();
-    const BrdfSample b = sample_brdf<true>(wo, n, alb, met, it.rough, rnd, metallic_on, next);
-    const float3 nt = ps.throughput * b.value;
-    if (all_zero(nt)) {
-        ps.throughput = f3(0.0f);
-        ps.active = 0u;
-        return;
-    }
-    float lpdf = 0.0f;
-    bool first_nee = false;
-    if (mis) {
-        lpdf = env_pdf(P.env, next);
-        first_nee = ps.bounces == 1u && max3(nt) >= 1e-4f;
-        if (first_nee) nee_grad_bwd(C, ps, s, it);
-    }
-    float3 dep = ps.acc;
-    if (mis && first_nee) dep -= ps.em.contribution * mis_weight(ps.em.light_pdf, ps.em.scatter_pdf);
-    const float3 num = ps.acc_grad * dep;
-    const float3 dl = make_float3(b.value.x > kBrdfEps ? num.x / b.value.x : 0.0f,
-                                  b.value.y > kBrdfEps ? num.y / b.value.y : 0.0f,
-                                  b.value.z > kBrdfEps ? num.z / b.value.z : 0.0f);
-    s.d_albedo += dl * b.d_albedo;
-    s.d_rough += dot(dl, b.d_rough);
-    if (metallic_on) s.d_metal += dot(dl, b.d_metallic);
-    ps.pend_valid = dot(b.d_next_dir, b.d_next_dir) > 0.0f;
-    ps.pend_o = it.o;
-    ps.pend_d = it.d;
-    ps.pend_opacity = 1.0f - it.transmittance;
-    ps.pend_max_hit = it.last_hit;
-    ps.pend_dnext = b.d_next_dir;
-    ps.pend_bounces = ps.bounces;
-    if (!all_zero(s.d_albedo) || s.d_rough != 0.0f || s.d_metal != 0.0f)
-        replay_material_grad(C, B, ps.bounces > 1u, it.o, it.d, 1.0f - it.transmittance, it.last_hit, s.d_albedo,
-                             s.d_rough, s.d_metal);
-    ps.throughput = nt;
-    const float3 origin = it.pos + normalize_or_keep(next) * 2e-2f;
-    segment_reset(s, origin, next, 0.0f);
-    if (mis) {
-        s.scatter_pdf = b.pdf;
-        s.light_pdf = lpdf;
-    }
-}
-
+// backward (referenceBwdOptix.cu:27-74)
 __global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    Ctx C{P, stack, stack_t, ctr};
+    CtxT<kKBuf> C{P, stack, stack_t, ctr};
     unsigned x, y, z;
     if (launch_index(P, x, y, z)) {
         const size_t li = ((size_t)z * P.h + y) * P.w + x;
@@ -730,11 +105,12 @@ __global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
             if (P.flags & kMis) sample_nee(C, ps, s, rng);
             for (unsigned depth = 0; depth < ps.max_bounces && ps.active; ++depth) {
                 accumulate_light_bwd(C, B, ps, s);
-                pending_bwd(C, B, ps, s);
+                const auto run_replay = [&](const ReplayJob& j) { replay_material_grad(C, B, j); };
+                pending_bwd(ps, s, run_replay);
                 ps.active &= (unsigned)((depth + 1u < ps.max_bounces) && s.ivalid);
                 if (!ps.active) break;
                 ps.bounces = depth + 1u;
-                sample_next_bwd(C, B, ps, s, rng);
+                sample_next_bwd(C, ps, s, rng, run_replay);
                 if (max3(ps.throughput) < 1e-4f) break;
                 ++ctr.segments;
                 intersect_mark<true>(C, s, rng, nullptr);

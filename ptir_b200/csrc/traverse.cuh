@@ -20,7 +20,7 @@
 
 namespace ptir {
 
-constexpr int kKBuf = 16;            // hits per trace call (reference MaxNumHitPerTrace)
+constexpr int kKBuf = 16;            // reference MaxNumHitPerTrace; the kernels also build K = 8 and 32
 constexpr int kStackDepth = 64;      // traversal stack entries
 constexpr unsigned kNoHit = 0xFFFFFFFFu;
 constexpr float kFarT = 1e20f;
@@ -29,26 +29,29 @@ struct TraceCounters {
     unsigned segments, calls, candidates, accepted, env, replay, replay_accepted, nodes, leaves;
 };
 
-PTIR_DEV void kbuf_clear(float (&kt)[kKBuf], unsigned (&kid)[kKBuf]) {
+template <int K>
+PTIR_DEV void kbuf_clear(float (&kt)[K], unsigned (&kid)[K]) {
 #pragma unroll
-    for (int j = 0; j < kKBuf; ++j) {
+    for (int j = 0; j < K; ++j) {
         kt[j] = kFarT;
         kid[j] = kNoHit;
     }
 }
 
 // number of filled slots
-PTIR_DEV unsigned kbuf_count(const unsigned (&kid)[kKBuf]) {
+template <int K>
+PTIR_DEV unsigned kbuf_count(const unsigned (&kid)[K]) {
     unsigned c = 0;
 #pragma unroll
-    for (int j = 0; j < kKBuf; ++j) c += kid[j] != kNoHit ? 1u : 0u;
+    for (int j = 0; j < K; ++j) c += kid[j] != kNoHit ? 1u : 0u;
     return c;
 }
 
 // sorted insertion; an entry equal to an existing distance goes behind it
-PTIR_DEV void kbuf_insert(float (&kt)[kKBuf], unsigned (&kid)[kKBuf], float t, unsigned id) {
+template <int K>
+PTIR_DEV void kbuf_insert(float (&kt)[K], unsigned (&kid)[K], float t, unsigned id) {
 #pragma unroll
-    for (int j = 0; j < kKBuf; ++j) {
+    for (int j = 0; j < K; ++j) {
         const bool lt = t < kt[j];
         const float tt = kt[j];
         const unsigned ii = kid[j];
@@ -69,8 +72,9 @@ PTIR_DEV void slab(float3 lo, float3 hi, float3 o, float3 inv, float& t0, float&
 }
 
 // exact instance test of leaf record p
-PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[kKBuf],
-                        unsigned (&kid)[kKBuf]) {
+template <int K>
+PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
+                        unsigned (&kid)[K]) {
     const float4* rec = A.leaves + 4 * (size_t)p;
     const float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
     const float3 od = make_float3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w,
@@ -81,7 +85,7 @@ PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmi
     const float dd2 = dot(dd, dd);
     const float den = 1.0f / dd2;
     const float ts = -dot(od, dd) * den;
-    if (!(ts > tmin && ts < tend && ts < kt[kKBuf - 1])) return;
+    if (!(ts > tmin && ts < tend && ts < kt[K - 1])) return;
     // object-space unit box within [tmin, tend]
     const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float b0, b1;
@@ -93,10 +97,11 @@ PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmi
     kbuf_insert(kt, kid, ts, gid);
 }
 
-// Fill (kt, kid) with the nearest candidates of ray (o, d) in (tmin, tend).
+// Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
 // `stack` holds kStackDepth node indices, `stack_t` their entry distances.
-PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[kKBuf],
-                         unsigned (&kid)[kKBuf], int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
+template <int K>
+PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
+                         unsigned (&kid)[K], int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
     kbuf_clear(kt, kid);
     ++ctr.calls;
     if (A.n <= 0) return;
@@ -121,7 +126,7 @@ PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, flo
         r0 = fmaxf(r0, tmin);
         l1 = fminf(l1, tend);
         r1 = fminf(r1, tend);
-        const float cut = kt[kKBuf - 1];
+        const float cut = kt[K - 1];
         bool hl = l0 <= l1 && l0 <= cut;
         bool hr = r0 <= r1 && r0 <= cut;
         if (hl && left < 0) {
@@ -155,7 +160,7 @@ PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, flo
             bool found = false;
             while (sp > 0) {
                 --sp;
-                if (stack_t[sp] <= kt[kKBuf - 1]) {
+                if (stack_t[sp] <= kt[K - 1]) {
                     node = stack[sp];
                     found = true;
                     break;

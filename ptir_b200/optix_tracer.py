@@ -54,6 +54,9 @@ class OptixTracer:
         enable_metallic: bool,
         visualize_lights: bool = False,
         collect_counters: bool = True,
+        schedule: str = "wavefront",
+        chunk_tiles: int = 0,
+        kbuffer: int = 16,
     ):
         if pipeline not in ("reference",):
             raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
@@ -67,7 +70,8 @@ class OptixTracer:
         cfg = N.PtirConfig(
             float(particle_kernel_degree), float(particle_kernel_min_response), int(bool(particle_kernel_density_clamping)),
             self.sph_degree, int(bool(enable_normals)), int(bool(enable_hit_counts)), int(bool(enable_mis)),
-            int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)))
+            int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
+            N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer))
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:

@@ -48,11 +48,12 @@ def to_torch(s: dict, device="cuda") -> dict:
 
 
 def make_tracer(sph_degree=3, normals=True, hitcounts=True, mis=True, metallic=False, visualize=False,
-                kernel_degree=4, min_response=0.0113, clamping=True):
+                kernel_degree=4, min_response=0.0113, clamping=True, schedule="wavefront", chunk_tiles=0, kbuffer=16):
     from ptir_b200 import OptixTracer
 
     return OptixTracer("", "", "reference", "referenceBwd", "instances", kernel_degree, min_response, clamping,
-                       sph_degree, normals, hitcounts, mis, metallic, visualize)
+                       sph_degree, normals, hitcounts, mis, metallic, visualize, schedule=schedule,
+                       chunk_tiles=chunk_tiles, kbuffer=kbuffer)
 
 
 def gpu_trace(tr, S: dict, build=True, rebuild=True):

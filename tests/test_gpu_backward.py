@@ -29,7 +29,8 @@ def _rel_cos(a, b):
     dict(n=2000, w=48, h=40, spp=2, max_bounces=3),
     dict(n=3000, w=40, h=32, spp=2, max_bounces=4, env_hw=(16, 32)),
 ])
-def test_backward_matches_oracle(cuda_device, case):
+@pytest.mark.parametrize("schedule", ["wavefront", "megakernel"])
+def test_backward_matches_oracle(cuda_device, case, schedule):
     s = small_scene(**case)
     cfg = O.OracleConfig()
     ref, _, _ = O.trace(cfg, s, "f64")
@@ -40,7 +41,7 @@ def test_backward_matches_oracle(cuda_device, case):
                  material=rng.standard_normal(zhw + (5,)).astype(np.float32))
     mg_ref, eg_ref, _ = O.trace_bwd(cfg, s, ref, grads, "f64")
 
-    tr = make_tracer()
+    tr = make_tracer(schedule=schedule)
     S = to_torch(s)
     fwd = gpu_trace(tr, S)
     # replay from the oracle's forward outputs so both backward passes start from identical values
