@@ -11,6 +11,7 @@
 //   7. refit     bottom-up child boxes with arrival counters
 // A refit (rebuild == false, same n) redoes 1, 2, 5 and 7 in the stored leaf order.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cstring>
@@ -245,6 +246,59 @@ __global__ void k_refit(int n, const float4* __restrict__ box, const unsigned* _
     }
 }
 
+// 1 for binary internal nodes at even depth (the root included): the 4-wide nodes
+__global__ void k_even_depth(int n, const int* __restrict__ parent, unsigned* __restrict__ even) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int d = 0;
+    for (int p = parent[i]; p >= 0 && d < 4096; p = parent[p]) ++d;
+    even[i] = (d & 1) ? 0u : 1u;
+}
+
+// 4-wide node of binary node b (even depth): the boxes of its children, a leaf child taken as
+// is, an internal child replaced by its own two children
+__global__ void k_emit4(int n, const float4* __restrict__ nodes, const unsigned* __restrict__ even,
+                        const unsigned* __restrict__ slot4, float4* __restrict__ nodes4) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n - 1 || !even[b]) return;
+    float lx[4], ly[4], lz[4], hx[4], hy[4], hz[4];
+    int ch[4];
+    int cnt = 0;
+    auto add = [&](int c, float3 lo, float3 hi) {
+        lx[cnt] = lo.x; ly[cnt] = lo.y; lz[cnt] = lo.z;
+        hx[cnt] = hi.x; hy[cnt] = hi.y; hz[cnt] = hi.z;
+        ch[cnt] = c < 0 ? c : (int)slot4[c];
+        ++cnt;
+    };
+    auto expand = [&](int c, float3 lo, float3 hi) {
+        if (c < 0) {
+            add(c, lo, hi);
+            return;
+        }
+        const float4* nc = nodes + 4 * (size_t)c;
+        const float4 a = nc[0], q = nc[1], r = nc[2], e = nc[3];
+        add(__float_as_int(e.x), make_float3(a.x, a.y, a.z), make_float3(a.w, q.x, q.y));
+        add(__float_as_int(e.y), make_float3(q.z, q.w, r.x), make_float3(r.y, r.z, r.w));
+    };
+    const float4* nb = nodes + 4 * (size_t)b;
+    const float4 a = nb[0], q = nb[1], r = nb[2], e = nb[3];
+    expand(__float_as_int(e.x), make_float3(a.x, a.y, a.z), make_float3(a.w, q.x, q.y));
+    expand(__float_as_int(e.y), make_float3(q.z, q.w, r.x), make_float3(r.y, r.z, r.w));
+    for (int k = cnt; k < 4; ++k) {
+        lx[k] = ly[k] = lz[k] = hx[k] = hy[k] = hz[k] = 0.0f;
+        ch[k] = kNoChild;
+    }
+    float4* out = nodes4 + 8 * (size_t)slot4[b];
+    out[0] = make_float4(lx[0], lx[1], lx[2], lx[3]);
+    out[1] = make_float4(ly[0], ly[1], ly[2], ly[3]);
+    out[2] = make_float4(lz[0], lz[1], lz[2], lz[3]);
+    out[3] = make_float4(hx[0], hx[1], hx[2], hx[3]);
+    out[4] = make_float4(hy[0], hy[1], hy[2], hy[3]);
+    out[5] = make_float4(hz[0], hz[1], hz[2], hz[3]);
+    out[6] = make_float4(__int_as_float(ch[0]), __int_as_float(ch[1]), __int_as_float(ch[2]), __int_as_float(ch[3]));
+    out[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 template <class T>
 cudaError_t grow(T*& ptr, size_t count, cudaStream_t s) {
     if (ptr) {
@@ -293,6 +347,9 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
         PTIR_TRY(grow(st.nodes, 4 * (cap > 1 ? cap - 1 : 1), s));
         PTIR_TRY(grow(st.parent, 2 * cap, s));
         PTIR_TRY(grow(st.arrivals, cap, s));
+        PTIR_TRY(grow(st.even, cap, s));
+        PTIR_TRY(grow(st.slot4, cap, s));
+        PTIR_TRY(grow(st.nodes4, 8 * (cap > 1 ? cap - 1 : 1), s));
         st.capacity = cap;
         st.valid = false;
     }
@@ -317,8 +374,22 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
         size_t have = st.sort_temp_bytes;
         PTIR_TRY(cub::DeviceRadixSort::SortPairs(st.sort_temp, have, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, 63, s));
         if (n > 1) {
-            k_hierarchy<<<(unsigned)((n - 1 + T - 1) / T), T, 0, s>>>(n, st.keys[1], st.nodes, st.parent);
+            const unsigned iblocks = (unsigned)((n - 1 + T - 1) / T);
+            k_hierarchy<<<iblocks, T, 0, s>>>(n, st.keys[1], st.nodes, st.parent);
             PTIR_TRY(cudaGetLastError());
+            // which binary nodes become 4-wide nodes, and where they go
+            k_even_depth<<<iblocks, T, 0, s>>>(n, st.parent, st.even);
+            PTIR_TRY(cudaGetLastError());
+            size_t scan_need = 0;
+            PTIR_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_need, st.even, st.slot4, n - 1, s));
+            if (scan_need > st.scan_temp_bytes) {
+                if (st.scan_temp) PTIR_TRY(cudaFreeAsync(st.scan_temp, s));
+                st.scan_temp = nullptr;
+                PTIR_TRY(cudaMallocAsync(&st.scan_temp, scan_need, s));
+                st.scan_temp_bytes = scan_need;
+            }
+            size_t scan_have = st.scan_temp_bytes;
+            PTIR_TRY(cub::DeviceScan::ExclusiveSum(st.scan_temp, scan_have, st.even, st.slot4, n - 1, s));
         }
     }
     k_gather<<<blocks, T, 0, s>>>(n, st.ids[1], st.inst, st.leaves);
@@ -326,6 +397,8 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
     if (n > 1) {
         PTIR_TRY(cudaMemsetAsync(st.arrivals, 0, sizeof(unsigned) * (size_t)(n - 1), s));
         k_refit<<<blocks, T, 0, s>>>(n, st.box, st.ids[1], st.nodes, st.parent, st.arrivals);
+        PTIR_TRY(cudaGetLastError());
+        k_emit4<<<(unsigned)((n - 1 + T - 1) / T), T, 0, s>>>(n, st.nodes, st.even, st.slot4, st.nodes4);
         PTIR_TRY(cudaGetLastError());
     }
     st.valid = true;
@@ -350,6 +423,10 @@ void accel_free(AccelState& st) {
     rel(st.partial);
     rel(st.bounds);
     rel(st.sort_temp);
+    rel(st.even);
+    rel(st.slot4);
+    rel(st.nodes4);
+    rel(st.scan_temp);
     st = AccelState();
 }
 

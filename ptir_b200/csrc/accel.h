@@ -31,11 +31,16 @@ struct AccelState {
     unsigned* arrivals = nullptr;  // [n-1] refit arrival counters
     float4* partial = nullptr;  // [kReduceBlocks*2] per-block bounds
     float4* bounds = nullptr;   // [2] scene AABB
+    unsigned* even = nullptr;   // [n-1] 1 where a binary node sits at even depth (a 4-wide node)
+    unsigned* slot4 = nullptr;  // [n-1] index of that 4-wide node
+    float4* nodes4 = nullptr;   // [(n-1)*8] 4-wide nodes traversed by the tracer
+    void* scan_temp = nullptr;
+    size_t scan_temp_bytes = 0;
     void* sort_temp = nullptr;
     size_t sort_temp_bytes = 0;
     size_t capacity = 0;        // Gaussians the buffers can hold
 
-    AccelView view() const { return AccelView{nodes, leaves, bounds, valid ? n : 0}; }
+    AccelView view() const { return AccelView{nodes4, leaves, bounds, valid ? n : 0}; }
 };
 
 // Build (rebuild != 0 or topology unusable) or refit the structure from per-Gaussian

@@ -7,15 +7,19 @@
 
 namespace ptir {
 
-// Acceleration structure over the Gaussians' instance boxes: a binary LBVH whose internal
-// node i stores the AABBs of both children (so one 64-byte fetch tests two boxes) and whose
-// leaves are the Morton-ordered instance records.
-//   node  = 4 x float4: (L.lo.xyz, L.hi.x) (L.hi.yz, R.lo.xy) (R.lo.z, R.hi.xyz)
-//           (left, right, kmax(L), kmax(R)); a child c >= 0 is an internal node, c < 0 is leaf ~c.
+// Acceleration structure over the Gaussians' instance boxes. The LBVH is built binary and
+// traversed 4-wide: every binary node at even depth becomes a 4-wide node holding the boxes of
+// its (up to four) grandchildren, so one 128-byte fetch tests four boxes.
+//   node4 = 8 x float4: lo.x[4] lo.y[4] lo.z[4] hi.x[4] hi.y[4] hi.z[4] child[4] (unused);
+//           a child c >= 0 is a 4-wide node, kNoChild an empty slot, any other c < 0 leaf ~c.
 //   leaf  = 4 x float4: rows of the world->instance affine map [A | b] (A = diag(1/k) R^T,
 //           b = -A mu, k = kernel support scale per axis), then (gaussian id, kmax, 0, 0).
+// (The binary nodes, 4 x float4 each: (L.lo.xyz, L.hi.x) (L.hi.yz, R.lo.xy) (R.lo.z, R.hi.xyz)
+//  (left, right, -, -), are kept for refits.)
+constexpr int kNoChild = (int)0x80000000;
+
 struct AccelView {
-    const float4* nodes;
+    const float4* nodes;  // 4-wide nodes
     const float4* leaves;
     const float4* bounds;  // [2]: scene AABB lo.xyz, hi.xyz (union of the instance AABBs)
     int n;                 // number of Gaussians (leaves)

@@ -116,45 +116,75 @@ PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, flo
     int node = 0;
     while (true) {
         ++ctr.nodes;
-        const float4* nd = A.nodes + 4 * (size_t)node;
-        const float4 a = __ldg(nd + 0), b = __ldg(nd + 1), c = __ldg(nd + 2), e = __ldg(nd + 3);
-        const int left = __float_as_int(e.x), right = __float_as_int(e.y);
-        float l0, l1, r0, r1;
-        slab(make_float3(a.x, a.y, a.z), make_float3(a.w, b.x, b.y), o, inv, l0, l1);
-        slab(make_float3(b.z, b.w, c.x), make_float3(c.y, c.z, c.w), o, inv, r0, r1);
-        l0 = fmaxf(l0, tmin);
-        r0 = fmaxf(r0, tmin);
-        l1 = fminf(l1, tend);
-        r1 = fminf(r1, tend);
-        const float cut = kt[K - 1];
-        bool hl = l0 <= l1 && l0 <= cut;
-        bool hr = r0 <= r1 && r0 <= cut;
-        if (hl && left < 0) {
-            ++ctr.leaves;
-            test_leaf(A, ~left, o, d, tmin, tend, kt, kid);
-            hl = false;
-        }
-        if (hr && right < 0) {
-            ++ctr.leaves;
-            test_leaf(A, ~right, o, d, tmin, tend, kt, kid);
-            hr = false;
-        }
-        if (hl && hr) {
+        const float4* nd = A.nodes + 8 * (size_t)node;
+        const float4 lx = __ldg(nd + 0), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
+        const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5), cc = __ldg(nd + 6);
+        const float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, lya[4] = {ly.x, ly.y, ly.z, ly.w}, lza[4] = {lz.x, lz.y, lz.z, lz.w};
+        const float hxa[4] = {hx.x, hx.y, hx.z, hx.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
+        const int ch[4] = {__float_as_int(cc.x), __float_as_int(cc.y), __float_as_int(cc.z), __float_as_int(cc.w)};
+        float t0[4], key[4];
+        bool hit[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            float a, b;
+            slab(make_float3(lxa[k], lya[k], lza[k]), make_float3(hxa[k], hya[k], hza[k]), o, inv, a, b);
+            a = fmaxf(a, tmin);
+            b = fminf(b, tend);
+            t0[k] = a;
             // nearer middle of the clipped interval first: boxes that contain the origin all
             // enter at tmin, their extent along the ray tells them apart
-            const bool lfirst = (l0 + l1) <= (r0 + r1);
-            if (sp >= kStackDepth) {
+            key[k] = a + b;
+            hit[k] = ch[k] != kNoChild && a <= b && a <= kt[K - 1];
+        }
+        // leaf children: one test call site, looping over the hit mask
+        unsigned leaves = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) leaves |= (hit[k] && ch[k] < 0) ? (1u << k) : 0u;
+        while (leaves) {
+            const int k = __ffs(leaves) - 1;
+            leaves &= leaves - 1;
+            const int c = k == 0 ? ch[0] : (k == 1 ? ch[1] : (k == 2 ? ch[2] : ch[3]));
+            ++ctr.leaves;
+            test_leaf(A, ~c, o, d, tmin, tend, kt, kid);
+        }
+        // the internal children still in front of the K-th distance: descend into the nearest,
+        // push the others farthest first so that the nearest of them is popped first
+        int best = -1;
+        float bkey = 3.0e38f;
+        unsigned inner = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const bool h = hit[k] && ch[k] >= 0 && t0[k] <= kt[K - 1];
+            inner |= h ? (1u << k) : 0u;
+            if (h && key[k] < bkey) {
+                bkey = key[k];
+                best = k;
+            }
+        }
+        if (best >= 0) {
+            inner &= ~(1u << best);
+            const int np = __popc(inner);
+            if (sp + np > kStackDepth) {
                 atomicOr(err, kErrStackOverflow);
                 break;
             }
-            stack[sp] = lfirst ? right : left;
-            stack_t[sp] = lfirst ? r0 : l0;
-            ++sp;
-            node = lfirst ? left : right;
-        } else if (hl) {
-            node = left;
-        } else if (hr) {
-            node = right;
+            while (inner) {
+                // farthest remaining first
+                int far = -1;
+                float fkey = -3.0e38f;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if ((inner >> k) & 1u && key[k] > fkey) {
+                        fkey = key[k];
+                        far = k;
+                    }
+                }
+                inner &= ~(1u << far);
+                stack[sp] = far == 0 ? ch[0] : (far == 1 ? ch[1] : (far == 2 ? ch[2] : ch[3]));
+                stack_t[sp] = far == 0 ? t0[0] : (far == 1 ? t0[1] : (far == 2 ? t0[2] : t0[3]));
+                ++sp;
+            }
+            node = best == 0 ? ch[0] : (best == 1 ? ch[1] : (best == 2 ? ch[2] : ch[3]));
         } else {
             // pop the next subtree that can still hold a candidate nearer than the K-th
             bool found = false;
