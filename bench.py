@@ -100,11 +100,11 @@ class Setup:
         e = lambda *s, dt=torch.float32: torch.empty(s, dtype=dt, device=device)  # noqa: E731
         self.lights = (e(0, 9), e(5, 0), e(0, 3), e(0, 3, dt=torch.int32), e(0, 8), e(3, 0))
 
-    def tracer(self):
+    def tracer(self, **kw):
         from ptir_b200 import OptixTracer
 
         return OptixTracer("", "", "reference", "referenceBwd", "instances", 4, 0.0113, True, 3, True, True, True,
-                           False, False)
+                           False, False, **kw)
 
     def trace(self, tr, material=None, ray_ori=None, ray_dir=None, frame=0):
         return tr.trace(frame, self.t2w, self.ray_ori if ray_ori is None else ray_ori,
@@ -172,6 +172,39 @@ def _clock_summary(lines: list):
 
 
 # ------------------------------------------------------------------------------------------
+STAGES = ("intersect", "shadow", "replay", "shading", "megakernel", "sort")
+KERNEL_OF_STAGE = {"intersect": "k_wf_trace", "shadow": "k_wf_shadow", "replay": "k_wb_replay",
+                   "shading": "k_wf_camera/primary/bounce", "megakernel": "k_trace_fwd/k_trace_bwd",
+                   "sort": "k_wf_sort_keys + CUB radix sort"}
+ACCEL_KERNELS_PER_BUILD = 9  # k_prep, k_bounds_partial, k_bounds_final, k_morton, k_hierarchy, k_even_depth,
+#                              k_gather, k_refit, k_emit4 (plus CUB's radix-sort and scan kernels)
+
+
+def stage_bytes(stage: str, c: dict, rec: dict) -> float:
+    """Algorithmic HBM bytes of one stage's work from its device counters: per segment 24 B of
+    ray, a geometry record per candidate, and per composited hit the material, SH and shading
+    normal records (`rec`: 48 / 20 / 192 / 12 B in FP32 storage, half in 16-bit storage); a replay
+    writes 20 B of material gradient per hit. BVH node fetches are implementation overhead and
+    not counted."""
+    hit = rec["mat"] + rec["sh"] + rec["nrm"]
+    if stage == "intersect":
+        return 24.0 * c["segments"] + rec["geo"] * c["candidates"] + hit * c["accepted"]
+    if stage == "shadow":
+        return 24.0 * c["segments"] + rec["geo"] * c["candidates"]
+    if stage == "replay":
+        return 24.0 * c["replay"] + rec["geo"] * c["candidates"] + 40.0 * c["replay_accepted"]
+    if stage == "shading":
+        return 64.0 * c["env_lookups"]
+    if stage == "sort":
+        return 36.0 * c["segments"]
+    return 24.0 * c["segments"] + rec["geo"] * c["candidates"] + hit * c["accepted"] + 64.0 * c["env_lookups"]
+
+
+def record_bytes(storage: str) -> dict:
+    f = 2 if storage in ("bf16", "fp16") else 1
+    return {"geo": 48 // f, "mat": 20 // f, "sh": 192 // f, "nrm": 12 // f}
+
+
 def algorithmic_bytes(fc: dict, bc: dict, samples: int):
     """Per-launch algorithmic HBM bytes of the forward and backward kernels.
 
@@ -191,7 +224,7 @@ def run_ours(args, rank, world, device):
     import torch.distributed as dist
 
     S = Setup(workload_of(args), rank, device)
-    tr = S.tracer()
+    tr = S.tracer(collect_timings=True, storage=args.storage)
     stream = torch.cuda.current_stream()
     # target image: the same scene with albedo perturbed by N(0, 0.02)
     gen = torch.Generator(device="cpu").manual_seed(1234)
@@ -224,19 +257,22 @@ def run_ours(args, rank, world, device):
             pdist.allreduce_gradients([mg, eg])
         return loss
 
-    # warm-up (also reads the deterministic per-launch counters)
+    # warm-up (also reads the deterministic per-launch counters, in total and per stage)
     fc = bc = None
+    fcs, bcs = {}, {}
     for i in range(args.warmup):
         tr.build_bvh(S.pos, S.rot, S.scl, S.dns, True, True)
         fwd = S.trace(tr)
         if i == 0:
             fc = tr.counters()
+            fcs = {st: tr.counters(st) for st in STAGES}
         if not hasattr(S, "_zeros"):
             S.prepare_grads(fwd)
         diff = fwd[10] - target
         S.trace_bwd(tr, fwd, torch.sign(diff) * (1.0 / diff.numel()))
         if i == 0:
             bc = tr.counters()
+            bcs = {st: tr.counters(st) for st in STAGES}
         del fwd
     torch.cuda.synchronize()
     status = tr.device_status()
@@ -248,6 +284,7 @@ def run_ours(args, rank, world, device):
     sampler = threading.Thread(target=_clock_sampler, args=(clock_lines, stop, torch.cuda.current_device()), daemon=True)
     sampler.start()
     time.sleep(0.3)
+    tr.stage_times()  # forget the warm-up launches
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
@@ -263,6 +300,7 @@ def run_ours(args, rank, world, device):
     stop.set()
     sampler.join(timeout=10)
     ms_total = t0.elapsed_time(t1)
+    stage_t = tr.stage_times()  # {stage: (ms, launches)} over the timed steps
     fwd_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
     bwd_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
 
@@ -303,13 +341,19 @@ def run_ours(args, rank, world, device):
     if rank != 0:
         return None
     ms_step = ms_total / args.steps
-    fwd_b, bwd_b = algorithmic_bytes(fc, bc, S.samples)
-    dom = "k_trace_bwd" if bwd_ms >= fwd_ms else "k_trace_fwd"
-    dom_bytes, dom_ms = (bwd_b, bwd_ms) if bwd_ms >= fwd_ms else (fwd_b, fwd_ms)
+    # the dominant kernel: the stage with the most device time; its algorithmic bytes per launch
+    # (forward + backward work of the stage per step / its launches per step) over its mean launch time
+    dom = max(STAGES, key=lambda st: stage_t[st][0])
+    dom_ms_total, dom_launches = stage_t[dom]
+    rec = record_bytes(args.storage)
+    dom_bytes_step = stage_bytes(dom, fcs[dom], rec) + stage_bytes(dom, bcs[dom], rec)
+    launches_step = dom_launches / args.steps
+    dom_bytes = dom_bytes_step / launches_step
+    dom_ms = dom_ms_total / dom_launches
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     w, h, spp = S.wl.views[0]
-    launches_per_step = 9  # k_prep, k_bounds_partial, k_bounds_final, k_morton, k_hierarchy, k_gather, k_refit, k_trace_fwd, k_trace_bwd
+    launches_per_step = ACCEL_KERNELS_PER_BUILD + sum(n for _, n in stage_t.values()) / args.steps
     res = {
         "metric": METRIC,
         "value": total_segs / (ms_step * 1e-3),
@@ -323,19 +367,21 @@ def run_ours(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": S.wl.name, "gaussians": S.wl.n, "views_per_gpu": len(S.wl.views), "resolution": [w, h],
+        "config": {"workload": S.wl.name, "storage": args.storage, "gaussians": S.wl.n, "views_per_gpu": len(S.wl.views), "resolution": [w, h],
                    "spp": spp, "max_bounces": S.wl.max_bounces, "env": list(S.wl.env_hw),
                    "samples_per_gpu": S.samples, "segments_per_step_per_gpu": segs,
                    "step": "bvh rebuild + forward + L1 loss grad + adjoint" + (" + grad all-reduce" if world > 1 else ""),
                    "l2": "inputs larger than L2 (scene + BVH records ~400 MB)", "parallelism": f"dp{world} over views"},
-        "kernels_ms": {"k_trace_fwd": fwd_ms, "k_trace_bwd": bwd_ms},
-        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
-                     "algorithmic_bytes_per_launch": dom_bytes},
-        "counters": {"forward": fc, "backward": bc},
+        "pass_ms": {"forward": fwd_ms, "backward": bwd_ms},
+        "stages_ms_per_step": {KERNEL_OF_STAGE[st]: stage_t[st][0] / args.steps for st in STAGES if stage_t[st][1]},
+        "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom], "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
+                     "launches_per_step": launches_step},
+        "counters": {"forward": fc, "backward": bc, "forward_by_stage": fcs, "backward_by_stage": bcs},
         "e2e": {"value": total_segs / (e2e_ms * 1e-3), "unit": "segments/s",
                 "h2d_bytes_per_step": int(S.ray_ori.numel() * 4 * 2), "d2h_bytes_per_step": 4, "ms_per_step": e2e_ms},
-        "gpu_launches": launches_per_step * args.steps,
+        "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": _clock_summary(clock_lines),
     }
     return res, S
@@ -398,6 +444,8 @@ def main():
     ap.add_argument("--res", default=None, help="WxH")
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--storage", default="fp32", choices=("fp32", "bf16", "fp16"),
+                    help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 

@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define PTIR_ABI_VERSION 1
+#define PTIR_ABI_VERSION 2
 
 enum {
     PTIR_OK = 0,
@@ -67,7 +67,18 @@ typedef struct ptir_config {
     int32_t chunk_tiles;          /* wavefront: 8x4 pixel tiles per chunk of paths (0 = default 131072) */
     int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16). The
                                      hits are composited in the same order for every size. */
+    int32_t refill_lanes;         /* wavefront intersection: waiting lanes, 1..32, before a warp refills (0 = 32) */
+    int32_t block_size;           /* wavefront: threads per block, 64, 128 or 256 (0 = 128) */
+    int32_t collect_timings;      /* record CUDA events around every kernel launch (ptir_get_stage_times) */
+    int32_t ray_order;            /* wavefront bounce rays: 0 = intersected in (direction octant, origin cell)
+                                     order (default), 1 = in queue order; results are the same */
+    int32_t storage;              /* attribute storage: PTIR_STORAGE_FP32 (the caller's tensors are read as
+                                     they are), _BF16 or _FP16 (geometry, material, shading normal and SH
+                                     rounded to nearest even once per call and by build_bvh; arithmetic
+                                     stays FP32) */
 } ptir_config;
+
+enum { PTIR_STORAGE_FP32 = 0, PTIR_STORAGE_BF16 = 1, PTIR_STORAGE_FP16 = 2 };
 
 enum { PTIR_SCHEDULE_WAVEFRONT = 0, PTIR_SCHEDULE_MEGAKERNEL = 1 };
 
@@ -147,6 +158,23 @@ typedef struct ptir_counters {
     uint64_t leaf_tests;      /* exact instance tests */
 } ptir_counters;
 
+/* The kernels of a trace, for ptir_get_stage_counters / ptir_get_stage_times. */
+enum {
+    PTIR_STAGE_INTERSECT = 0,  /* wavefront: primary and bounce segments (traversal + compositing) */
+    PTIR_STAGE_SHADOW = 1,     /* wavefront: NEE shadow rays */
+    PTIR_STAGE_REPLAY = 2,     /* wavefront backward: material-gradient re-traversals */
+    PTIR_STAGE_SHADING = 3,    /* wavefront: camera rays, primary outputs, light gathering, BRDF sampling */
+    PTIR_STAGE_MEGAKERNEL = 4, /* megakernel schedule: the whole-path kernel */
+    PTIR_STAGE_SORT = 5,       /* wavefront: ray-order keys and their radix sort */
+    PTIR_NUM_STAGES = 6
+};
+
+/* Device time of each stage's launches since the previous read (collect_timings = 1). */
+typedef struct ptir_stage_times {
+    double ms[PTIR_NUM_STAGES];          /* summed launch intervals, CUDA events on the launch stream */
+    uint64_t launches[PTIR_NUM_STAGES];  /* launches timed */
+} ptir_stage_times;
+
 int ptir_abi_version(void);
 
 /* OptixTracer(path, cuda_path, pipeline, backwardPipeline, primitive, ...) */
@@ -168,6 +196,12 @@ int ptir_trace_bwd(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_
 
 /* Counters of the last launch; synchronises `stream`. */
 int ptir_get_counters(ptir_tracer* tracer, ptir_counters* out, void* stream);
+
+/* Counters of one stage (PTIR_STAGE_*) of the last launch; synchronises `stream`. */
+int ptir_get_stage_counters(ptir_tracer* tracer, int32_t stage, ptir_counters* out, void* stream);
+
+/* Stage times recorded since the previous call, then cleared; waits for the recorded events. */
+int ptir_get_stage_times(ptir_tracer* tracer, ptir_stage_times* out);
 
 /* Bounded-loop status word of the last launches (0 = clean); synchronises `stream` and clears it. */
 int ptir_device_status(ptir_tracer* tracer, uint32_t* status_word, void* stream);

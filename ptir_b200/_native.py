@@ -35,7 +35,20 @@ class PtirConfig(C.Structure):
         ("schedule", C.c_int32),
         ("chunk_tiles", C.c_int32),
         ("kbuffer", C.c_int32),
+        ("refill_lanes", C.c_int32),
+        ("block_size", C.c_int32),
+        ("collect_timings", C.c_int32),
+        ("ray_order", C.c_int32),
+        ("storage", C.c_int32),
     ]
+
+
+STORAGES = {"fp32": 0, "bf16": 1, "fp16": 2}
+STAGES = ("intersect", "shadow", "replay", "shading", "megakernel", "sort")
+
+
+class PtirStageTimes(C.Structure):
+    _fields_ = [("ms", C.c_double * len(STAGES)), ("launches", C.c_uint64 * len(STAGES))]
 
 
 SCHEDULES = {"wavefront": 0, "megakernel": 1}
@@ -88,7 +101,8 @@ class PtirCounters(C.Structure):
 
 
 EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", "ptir_trace", "ptir_trace_bwd",
-           "ptir_get_counters", "ptir_device_status", "ptir_scene_bounds", "ptir_debug_accel", "ptir_last_error")
+           "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_device_status",
+           "ptir_scene_bounds", "ptir_debug_accel", "ptir_last_error")
 
 
 def lib_path() -> str:
@@ -120,6 +134,10 @@ def load(build_if_missing: bool = True):
     L.ptir_trace_bwd.restype = C.c_int
     L.ptir_get_counters.argtypes = [C.c_void_p, P(PtirCounters), C.c_void_p]
     L.ptir_get_counters.restype = C.c_int
+    L.ptir_get_stage_counters.argtypes = [C.c_void_p, C.c_int32, P(PtirCounters), C.c_void_p]
+    L.ptir_get_stage_counters.restype = C.c_int
+    L.ptir_get_stage_times.argtypes = [C.c_void_p, P(PtirStageTimes)]
+    L.ptir_get_stage_times.restype = C.c_int
     L.ptir_device_status.argtypes = [C.c_void_p, P(C.c_uint32), C.c_void_p]
     L.ptir_device_status.restype = C.c_int
     L.ptir_scene_bounds.argtypes = [C.c_void_p, P(C.c_float), C.c_void_p]

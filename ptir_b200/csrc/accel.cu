@@ -4,7 +4,7 @@
 //   1. prep      per Gaussian: kernel support scale, world->instance map, instance AABB
 //                (the instance transform of threedgptir_tracer/src/particlePrimitives.cu:543-610)
 //   2. bounds    scene AABB = union of the instance AABBs (two-pass reduction)
-//   3. morton    63-bit Morton key of the AABB centre within the scene bounds
+//   3. morton    60-bit extended Morton key: AABB centre and size
 //   4. sort      key/id radix sort (CUB)
 //   5. gather    leaf records in key order
 //   6. hierarchy internal nodes from the sorted keys (ties broken by position)
@@ -20,6 +20,7 @@
 
 #include "../../include/ptir_b200.h"
 #include "accel.h"
+#include "storage.cuh"
 #include "vecmath.cuh"
 
 namespace ptir {
@@ -48,11 +49,13 @@ __global__ void k_prep(int n, const float* __restrict__ pos, const float* __rest
                        float4* __restrict__ box) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n) return;
-    const float4 q = make_float4(rot[4 * g], rot[4 * g + 1], rot[4 * g + 2], rot[4 * g + 3]);
+    // the attributes as the tracer stores them (rounded in 16-bit storage)
+    const auto in = [&](const float* v, int i) { return round_storage(opt.storage, v[i]); };
+    const float4 q = make_float4(in(rot, 4 * g), in(rot, 4 * g + 1), in(rot, 4 * g + 2), in(rot, 4 * g + 3));
     const Mat3 R = quat_r(q);
-    const float ks = support_scale(dns[g], opt.min_response, opt.density_clamping, opt.kernel_degree);
-    const float3 k = make_float3(scl[3 * g], scl[3 * g + 1], scl[3 * g + 2]) * ks;
-    const float3 mu = make_float3(pos[3 * g], pos[3 * g + 1], pos[3 * g + 2]);
+    const float ks = support_scale(in(dns, g), opt.min_response, opt.density_clamping, opt.kernel_degree);
+    const float3 k = make_float3(in(scl, 3 * g), in(scl, 3 * g + 1), in(scl, 3 * g + 2)) * ks;
+    const float3 mu = make_float3(in(pos, 3 * g), in(pos, 3 * g + 1), in(pos, 3 * g + 2));
     // world = R diag(k) obj + mu  =>  obj = diag(1/k) R^T (world - mu)
     const float3 a0 = make_float3(R.r0.x, R.r1.x, R.r2.x) * (1.0f / k.x);
     const float3 a1 = make_float3(R.r0.y, R.r1.y, R.r2.y) * (1.0f / k.y);
@@ -129,16 +132,23 @@ __global__ void k_bounds_final(int parts, const float4* __restrict__ partial, fl
     }
 }
 
-// spread the low 21 bits of v to every third bit
-__device__ unsigned long long spread3(unsigned long long v) {
-    v &= 0x1FFFFFull;
-    v = (v | (v << 32)) & 0x001F00000000FFFFull;
-    v = (v | (v << 16)) & 0x001F0000FF0000FFull;
-    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
-    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
-    v = (v | (v << 2)) & 0x1249249249249249ull;
+// spread the low 16 bits of v to every fourth bit
+__device__ unsigned long long spread4(unsigned long long v) {
+    v &= 0xFFFFull;
+    v = (v | (v << 24)) & 0x000000FF000000FFull;
+    v = (v | (v << 12)) & 0x000F000F000F000Full;
+    v = (v | (v << 6)) & 0x0303030303030303ull;
+    v = (v | (v << 3)) & 0x1111111111111111ull;
     return v;
 }
+
+// Extended Morton key (Vinkler, Bittner and Havran 2017, "Extended Morton Codes for High
+// Performance Bounding Volume Hierarchy Construction"): the AABB centre within the scene bounds
+// and the AABB diagonal relative to the scene diagonal (weighted by kSizeWeight) as a fourth
+// axis, 15 bits each, interleaved x y z size from the top. Large Gaussians then group apart
+// from small neighbours instead of inflating every ancestor of a small-Gaussian subtree.
+constexpr float kSizeWeight = 0.5f;
+constexpr int kKeyBits = 60;
 
 __global__ void k_morton(int n, const float4* __restrict__ box, const float4* __restrict__ bounds,
                          unsigned long long* __restrict__ keys, unsigned* __restrict__ ids) {
@@ -148,11 +158,14 @@ __global__ void k_morton(int n, const float4* __restrict__ box, const float4* __
     const float4 lo = bounds[0], hi = bounds[1];
     const float3 c = make_float3(0.5f * (a.x + b.x), 0.5f * (a.y + b.y), 0.5f * (a.z + b.z));
     const float3 ext = make_float3(fmaxf(hi.x - lo.x, 1e-30f), fmaxf(hi.y - lo.y, 1e-30f), fmaxf(hi.z - lo.z, 1e-30f));
-    const float scale = 2097151.0f;  // 2^21 - 1
+    const float3 e = make_float3(b.x - a.x, b.y - a.y, b.z - a.z);
+    const float scale = 32767.0f;  // 2^15 - 1
     const unsigned long long qx = (unsigned long long)fminf(fmaxf((c.x - lo.x) / ext.x, 0.0f) * scale, scale);
     const unsigned long long qy = (unsigned long long)fminf(fmaxf((c.y - lo.y) / ext.y, 0.0f) * scale, scale);
     const unsigned long long qz = (unsigned long long)fminf(fmaxf((c.z - lo.z) / ext.z, 0.0f) * scale, scale);
-    keys[g] = (spread3(qx) << 2) | (spread3(qy) << 1) | spread3(qz);
+    const float size = kSizeWeight * sqrtf(dot(e, e) / dot(ext, ext));
+    const unsigned long long qs = (unsigned long long)fminf(fmaxf(size, 0.0f) * scale, scale);
+    keys[g] = (spread4(qx) << 3) | (spread4(qy) << 2) | (spread4(qz) << 1) | spread4(qs);
     ids[g] = (unsigned)g;
 }
 
@@ -364,7 +377,7 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
         k_morton<<<blocks, T, 0, s>>>(n, st.box, st.bounds, st.keys[0], st.ids[0]);
         PTIR_TRY(cudaGetLastError());
         size_t need = 0;
-        PTIR_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, 63, s));
+        PTIR_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, kKeyBits, s));
         if (need > st.sort_temp_bytes) {
             if (st.sort_temp) PTIR_TRY(cudaFreeAsync(st.sort_temp, s));
             st.sort_temp = nullptr;
@@ -372,7 +385,7 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
             st.sort_temp_bytes = need;
         }
         size_t have = st.sort_temp_bytes;
-        PTIR_TRY(cub::DeviceRadixSort::SortPairs(st.sort_temp, have, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, 63, s));
+        PTIR_TRY(cub::DeviceRadixSort::SortPairs(st.sort_temp, have, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, kKeyBits, s));
         if (n > 1) {
             const unsigned iblocks = (unsigned)((n - 1 + T - 1) / T);
             k_hierarchy<<<iblocks, T, 0, s>>>(n, st.keys[1], st.nodes, st.parent);

@@ -15,6 +15,7 @@ struct AccelBuildOptions {
     float kernel_degree;     // generalized-Gaussian degree of the particle kernel
     float min_response;      // kernel support ends where the (clamped) response reaches this
     int density_clamping;    // adaptive support: the response threshold is divided by the density
+    unsigned storage;        // attribute storage (storage.cuh): inputs are rounded to it first
 };
 
 // Device buffers of one acceleration structure; grown on demand, never shrunk.

@@ -7,14 +7,28 @@
 #include "../../include/ptir_b200.h"
 #include "accel.h"
 #include "device_types.h"
+#include "stages.h"
+#include "storage.cuh"
 #include "wavefront.h"
+
+static_assert((int)PTIR_STAGE_INTERSECT == (int)ptir::kStageIntersect &&
+                  (int)PTIR_STAGE_SHADOW == (int)ptir::kStageShadow &&
+                  (int)PTIR_STAGE_REPLAY == (int)ptir::kStageReplay &&
+                  (int)PTIR_STAGE_SHADING == (int)ptir::kStageShading &&
+                  (int)PTIR_STAGE_MEGAKERNEL == (int)ptir::kStageMegakernel &&
+                  (int)PTIR_STAGE_SORT == (int)ptir::kStageSort && (int)PTIR_NUM_STAGES == (int)ptir::kNumStages,
+              "stage numbering of the C ABI");
 
 struct ptir_tracer {
     ptir_config cfg;
     ptir::AccelState accel;
     ptir::WavefrontBuffers wave;
+    ptir::StageTimer timer;
+    uint4* hot = nullptr;     // 16-bit attribute records (storage != FP32)
+    uint4* cold = nullptr;
+    size_t attr_capacity = 0;  // Gaussians the record buffers hold
     unsigned* error_word = nullptr;
-    unsigned long long* counters = nullptr;
+    unsigned long long* counters = nullptr;  // [kNumStages][kNumCounters]
     std::string last_error;
 };
 
@@ -31,7 +45,24 @@ int cuda_fail(ptir_tracer* t, cudaError_t e, const char* what) {
 
 cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
-unsigned chunk_tiles_of(const ptir_config& c) { return c.chunk_tiles > 0 ? (unsigned)c.chunk_tiles : 131072u; }
+ptir::WavefrontTuning tuning_of(const ptir_config& c) {
+    ptir::WavefrontTuning w;
+    if (c.chunk_tiles > 0) w.chunk_tiles = (unsigned)c.chunk_tiles;
+    if (c.kbuffer > 0) w.kbuf = c.kbuffer;
+    if (c.refill_lanes > 0) w.refill_lanes = c.refill_lanes;
+    if (c.block_size > 0) w.block = c.block_size;
+    w.sort_rays = c.ray_order == 0;
+    return w;
+}
+
+constexpr size_t kCounterBytes = sizeof(unsigned long long) * ptir::kNumStages * ptir::kNumCounters;
+
+ptir::StageCtx stage_ctx(ptir_tracer* t) {
+    ptir::StageCtx sc;
+    sc.counters = t->cfg.collect_counters ? t->counters : nullptr;
+    sc.timer = &t->timer;
+    return sc;
+}
 
 unsigned flags_of(const ptir_config& c) {
     unsigned f = 0;
@@ -112,7 +143,55 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, ptir::TraceParams& p) {
     p.max_bounces = a->max_bounces;
     p.render_opts = a->sh_indirect ? 1u : 0u;
     p.error_word = t->error_word;
-    p.counters = t->cfg.collect_counters ? t->counters : nullptr;
+    p.counters = nullptr;  // per stage, set by the launchers (StageCtx)
+    return PTIR_OK;
+}
+
+// 16-bit storage: round and pack this call's attribute tensors into the tracer's records
+int pack_attributes(ptir_tracer* t, const ptir_trace_args* a, ptir::TraceParams& p, cudaStream_t s) {
+    if (t->cfg.storage == PTIR_STORAGE_FP32 || a->n <= 0) return PTIR_OK;
+    const int cold_stride = ptir::cold_stride_of(p.part.sph_stride);
+    if ((size_t)a->n > t->attr_capacity) {
+        cudaError_t e = cudaSuccess;
+        if (t->hot) e = cudaFreeAsync(t->hot, s);
+        if (e == cudaSuccess && t->cold) e = cudaFreeAsync(t->cold, s);
+        t->hot = t->cold = nullptr;
+        t->attr_capacity = 0;
+        if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&t->hot), sizeof(uint4) * 2 * (size_t)a->n, s);
+        if (e == cudaSuccess)
+            e = cudaMallocAsync(reinterpret_cast<void**>(&t->cold), sizeof(uint4) * cold_stride * (size_t)a->n, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "allocate attribute records");
+        t->attr_capacity = (size_t)a->n;
+    }
+    const cudaError_t e = ptir::launch_pack_attributes(a->n, a->particle_density, a->particle_material,
+                                                       a->particle_radiance, p.part.sph_stride,
+                                                       a->particle_shading_normal, (unsigned)t->cfg.storage, t->hot,
+                                                       t->cold, s);
+    if (e != cudaSuccess) return cuda_fail(t, e, "pack attributes");
+    p.part.storage = (unsigned)t->cfg.storage;
+    p.part.hot = t->hot;
+    p.part.cold = t->cold;
+    p.part.cold_stride = cold_stride;
+    return PTIR_OK;
+}
+
+int read_counters(ptir_tracer* t, int first, int last, ptir_counters* out, void* stream) {
+    unsigned long long h[ptir::kNumStages * ptir::kNumCounters];
+    cudaError_t e = cudaMemcpyAsync(h, t->counters, kCounterBytes, cudaMemcpyDeviceToHost, as_stream(stream));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
+    if (e != cudaSuccess) return cuda_fail(t, e, "read counters");
+    unsigned long long v[ptir::kNumCounters] = {};
+    for (int st = first; st < last; ++st)
+        for (int k = 0; k < ptir::kNumCounters; ++k) v[k] += h[st * ptir::kNumCounters + k];
+    out->segments = v[ptir::kCtrSegments];
+    out->trace_calls = v[ptir::kCtrTraceCalls];
+    out->candidates = v[ptir::kCtrCandidates];
+    out->accepted = v[ptir::kCtrAccepted];
+    out->env_lookups = v[ptir::kCtrEnvLookups];
+    out->replay = v[ptir::kCtrReplay];
+    out->replay_accepted = v[ptir::kCtrReplayAccepted];
+    out->node_visits = v[ptir::kCtrNodes];
+    out->leaf_tests = v[ptir::kCtrLeaves];
     return PTIR_OK;
 }
 
@@ -133,17 +212,25 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     if (config->schedule != PTIR_SCHEDULE_WAVEFRONT && config->schedule != PTIR_SCHEDULE_MEGAKERNEL) return PTIR_EINVAL;
     if (config->chunk_tiles < 0) return PTIR_EINVAL;
     if (!(config->kbuffer == 0 || config->kbuffer == 8 || config->kbuffer == 16 || config->kbuffer == 32)) return PTIR_EINVAL;
+    if (config->refill_lanes < 0 || config->refill_lanes > 32) return PTIR_EINVAL;
+    if (!(config->block_size == 0 || config->block_size == 64 || config->block_size == 128 || config->block_size == 256))
+        return PTIR_EINVAL;
+    if (config->ray_order != 0 && config->ray_order != 1) return PTIR_EINVAL;
+    if (config->storage != PTIR_STORAGE_FP32 && config->storage != PTIR_STORAGE_BF16 &&
+        config->storage != PTIR_STORAGE_FP16)
+        return PTIR_EINVAL;
     ptir_tracer* t = new ptir_tracer();
     t->cfg = *config;
+    t->timer.enabled = config->collect_timings != 0;
     if (cudaMalloc(&t->error_word, sizeof(unsigned)) != cudaSuccess ||
-        cudaMalloc(&t->counters, sizeof(unsigned long long) * ptir::kNumCounters) != cudaSuccess) {
+        cudaMalloc(&t->counters, kCounterBytes) != cudaSuccess) {
         cudaFree(t->error_word);
         cudaFree(t->counters);
         delete t;
         return PTIR_ECUDA;
     }
     cudaMemset(t->error_word, 0, sizeof(unsigned));
-    cudaMemset(t->counters, 0, sizeof(unsigned long long) * ptir::kNumCounters);
+    cudaMemset(t->counters, 0, kCounterBytes);
     *out = t;
     return PTIR_OK;
 }
@@ -155,6 +242,8 @@ void ptir_destroy(ptir_tracer* t) {
     ptir::wavefront_free(t->wave);
     cudaFree(t->error_word);
     cudaFree(t->counters);
+    cudaFree(t->hot);
+    cudaFree(t->cold);
     delete t;
 }
 
@@ -163,7 +252,8 @@ int ptir_build_bvh(ptir_tracer* t, const float* pos, const float* rot, const flo
     if (!t) return PTIR_EINVAL;
     if (n < 0) return fail(t, PTIR_EINVAL, "negative particle count");
     if (n > 0 && (!pos || !rot || !scl || !dns)) return fail(t, PTIR_EINVAL, "null particle pointer");
-    ptir::AccelBuildOptions opt{t->cfg.kernel_degree, t->cfg.kernel_min_response, t->cfg.density_clamping};
+    ptir::AccelBuildOptions opt{t->cfg.kernel_degree, t->cfg.kernel_min_response, t->cfg.density_clamping,
+                                (unsigned)t->cfg.storage};
     // the reference refits only when asked and allowed and the count is unchanged (optixTracer.cpp:646-649, 819-822)
     const bool do_rebuild = rebuild != 0 || allow_update == 0 || n != t->accel.n;
     std::string err;
@@ -184,13 +274,14 @@ int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_output
                          !o->pbr || !o->light || !o->pbr_components))
         return fail(t, PTIR_EINVAL, "every per-sample output buffer is required");
     cudaStream_t s = as_stream(stream);
+    if (pack_attributes(t, a, p, s) != PTIR_OK) return PTIR_ECUDA;
     cudaError_t e;
     if (o->visibility && a->n > 0) {
         e = cudaMemsetAsync(o->visibility, 0, sizeof(float) * (size_t)a->n, s);
         if (e != cudaSuccess) return cuda_fail(t, e, "clear visibility");
     }
-    if (p.counters) {
-        e = cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long) * ptir::kNumCounters, s);
+    if (t->cfg.collect_counters) {
+        e = cudaMemsetAsync(t->counters, 0, kCounterBytes, s);
         if (e != cudaSuccess) return cuda_fail(t, e, "clear counters");
     }
     ptir::FwdOutputs fo;
@@ -207,9 +298,10 @@ int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_output
     fo.light = o->light;
     fo.components = o->pbr_components;
     fo.visibility = o->visibility;
+    const ptir::StageCtx sc = stage_ctx(t);
     e = t->cfg.schedule == PTIR_SCHEDULE_MEGAKERNEL
-            ? ptir::launch_trace_fwd(p, fo, 128, s)
-            : ptir::launch_trace_fwd_wavefront(p, fo, t->wave, chunk_tiles_of(t->cfg), t->cfg.kbuffer, s);
+            ? ptir::launch_trace_fwd(p, fo, sc, s)
+            : ptir::launch_trace_fwd_wavefront(p, fo, t->wave, tuning_of(t->cfg), sc, s);
     if (e != cudaSuccess) return cuda_fail(t, e, "trace launch");
     return PTIR_OK;
 }
@@ -225,6 +317,7 @@ int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args
     if (launches > 0 && (!b->pbr || !b->light)) return fail(t, PTIR_EINVAL, "forward pbr and light are required");
     if (a->n > 0 && !o->particle_material_grad) return fail(t, PTIR_EINVAL, "particle_material_grad is required");
     cudaStream_t s = as_stream(stream);
+    if (pack_attributes(t, a, p, s) != PTIR_OK) return PTIR_ECUDA;
     cudaError_t e;
     if (a->n > 0) {
         e = cudaMemsetAsync(o->particle_material_grad, 0, sizeof(float) * 5 * (size_t)a->n, s);
@@ -235,8 +328,8 @@ int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args
         e = cudaMemsetAsync(o->environment_grad, 0, sizeof(float) * 4 * (size_t)p.env.w * p.env.h, s);
         if (e != cudaSuccess) return cuda_fail(t, e, "clear environment grad");
     }
-    if (p.counters) {
-        e = cudaMemsetAsync(t->counters, 0, sizeof(unsigned long long) * ptir::kNumCounters, s);
+    if (t->cfg.collect_counters) {
+        e = cudaMemsetAsync(t->counters, 0, kCounterBytes, s);
         if (e != cudaSuccess) return cuda_fail(t, e, "clear counters");
     }
     ptir::BwdInputs bi;
@@ -247,28 +340,34 @@ int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args
     bi.material_grad = b->material_grad;
     bi.particle_material_grad = o->particle_material_grad;
     bi.environment_grad = env ? o->environment_grad : nullptr;
+    const ptir::StageCtx sc = stage_ctx(t);
     e = t->cfg.schedule == PTIR_SCHEDULE_MEGAKERNEL
-            ? ptir::launch_trace_bwd(p, bi, 128, s)
-            : ptir::launch_trace_bwd_wavefront(p, bi, t->wave, chunk_tiles_of(t->cfg), t->cfg.kbuffer, s);
+            ? ptir::launch_trace_bwd(p, bi, sc, s)
+            : ptir::launch_trace_bwd_wavefront(p, bi, t->wave, tuning_of(t->cfg), sc, s);
     if (e != cudaSuccess) return cuda_fail(t, e, "trace_bwd launch");
     return PTIR_OK;
 }
 
 int ptir_get_counters(ptir_tracer* t, ptir_counters* out, void* stream) {
     if (!t || !out) return PTIR_EINVAL;
-    unsigned long long h[ptir::kNumCounters];
-    cudaError_t e = cudaMemcpyAsync(h, t->counters, sizeof(h), cudaMemcpyDeviceToHost, as_stream(stream));
-    if (e == cudaSuccess) e = cudaStreamSynchronize(as_stream(stream));
-    if (e != cudaSuccess) return cuda_fail(t, e, "read counters");
-    out->segments = h[ptir::kCtrSegments];
-    out->trace_calls = h[ptir::kCtrTraceCalls];
-    out->candidates = h[ptir::kCtrCandidates];
-    out->accepted = h[ptir::kCtrAccepted];
-    out->env_lookups = h[ptir::kCtrEnvLookups];
-    out->replay = h[ptir::kCtrReplay];
-    out->replay_accepted = h[ptir::kCtrReplayAccepted];
-    out->node_visits = h[ptir::kCtrNodes];
-    out->leaf_tests = h[ptir::kCtrLeaves];
+    return read_counters(t, 0, ptir::kNumStages, out, stream);
+}
+
+int ptir_get_stage_counters(ptir_tracer* t, int32_t stage, ptir_counters* out, void* stream) {
+    if (!t || !out || stage < 0 || stage >= ptir::kNumStages) return PTIR_EINVAL;
+    return read_counters(t, stage, stage + 1, out, stream);
+}
+
+int ptir_get_stage_times(ptir_tracer* t, ptir_stage_times* out) {
+    if (!t || !out) return PTIR_EINVAL;
+    double ms[ptir::kNumStages] = {};
+    unsigned long long n[ptir::kNumStages] = {};
+    const cudaError_t e = t->timer.collect(ms, n);
+    if (e != cudaSuccess) return cuda_fail(t, e, "read stage times");
+    for (int k = 0; k < ptir::kNumStages; ++k) {
+        out->ms[k] = ms[k];
+        out->launches[k] = n[k];
+    }
     return PTIR_OK;
 }
 

@@ -48,9 +48,13 @@ struct ParticleView {
     const float4* density;   // [n, 3] float4 = pos.xyz dns | quat wxyz | scale.xyz pad
     const float* material;   // [n, 5]
     const float* sph;        // [n, sph_stride]
-    const float* snrm;       // [n, 3] or null
+    const float* snrm;       // [n, 3] or null (also the "normals present" flag in 16-bit storage)
     int sph_stride;          // floats per particle (3 * max coefficients)
     int sph_degree;          // evaluation degree (<= max)
+    unsigned storage;        // Storage (storage.cuh): FP32 reads the four arrays above, else hot / cold
+    const uint4* hot;        // [n, 2] 16-bit geometry records
+    const uint4* cold;       // [n, cold_stride] 16-bit material / normal / SH records
+    int cold_stride;         // uint4 per cold record
 };
 
 struct TraceParams {
@@ -118,8 +122,9 @@ enum ErrorBits : unsigned {
     kErrLoopBound = 2u,
 };
 
-// launch helpers implemented in the .cu files
-cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, int block, cudaStream_t s);
-cudaError_t launch_trace_bwd(const TraceParams& p, const BwdInputs& b, int block, cudaStream_t s);
+// megakernel schedule (tracer.cu): one thread per path
+struct StageCtx;
+cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, const StageCtx& sc, cudaStream_t s);
+cudaError_t launch_trace_bwd(const TraceParams& p, const BwdInputs& b, const StageCtx& sc, cudaStream_t s);
 
 }  // namespace ptir

@@ -5,6 +5,7 @@
 #include "device_types.h"
 #include "pcg.cuh"
 #include "shading.cuh"
+#include "storage.cuh"
 #include "traverse.cuh"
 #include "vecmath.cuh"
 
@@ -97,19 +98,18 @@ PTIR_DEV float kernel_response(int degree, float d2) {
 }
 
 PTIR_DEV Response respond(const TraceParams& P, unsigned id, float3 o, float3 d, float& density) {
-    const float4* rec = P.part.density + 3 * (size_t)id;
-    const float4 a = __ldg(rec + 0), q = __ldg(rec + 1), c = __ldg(rec + 2);
+    const Geom g = load_geom(P.part, id);
     Response r;
-    r.rt = quat_rt(q);
-    r.scl = make_float3(c.x, c.y, c.z);
-    const float3 is = make_float3(1.0f / c.x, 1.0f / c.y, 1.0f / c.z);
-    r.gro = is * mul_rows(r.rt, o - make_float3(a.x, a.y, a.z));
+    r.rt = quat_rt(g.quat);
+    r.scl = g.scl;
+    const float3 is = make_float3(1.0f / g.scl.x, 1.0f / g.scl.y, 1.0f / g.scl.z);
+    r.gro = is * mul_rows(r.rt, o - g.pos);
     r.grd = normalize_or_keep(is * mul_rows(r.rt, d));
     const float3 cr = cross(r.grd, r.gro);
     r.d2 = dot(cr, cr);
     r.gres = kernel_response(P.kernel_degree, r.d2);
-    density = a.w;
-    r.alpha = fminf(0.99f, r.gres * a.w);
+    density = g.dns;
+    r.alpha = fminf(0.99f, r.gres * g.dns);
     return r;
 }
 
@@ -117,35 +117,58 @@ PTIR_DEV Response respond(const TraceParams& P, unsigned id, float3 o, float3 d,
 // the ray (pathTracer.cuh:115-128)
 PTIR_DEV bool self_occluded(const TraceParams& P, float t, unsigned id, float3 d) {
     if (t > (1e-1f - 2e-2f) || P.part.snrm == nullptr) return false;
-    return dot(ld3(P.part.snrm + 3 * (size_t)id), d) > 0.1f;
+    return dot(load_snrm(P.part, id), d) > 0.1f;
 }
 
+// SH coefficient k (0..15) of one Gaussian as an RGB triple: FP32 rows of the caller's tensor ...
+struct ShRowF32 {
+    const float* c;
+    __device__ __forceinline__ float3 operator()(int k) const { return ld3(c + 3 * k); }
+};
+
+// ... or the 16-bit SH of a cold record
+struct ShRow16 {
+    const unsigned short* c;
+    unsigned storage;
+    __device__ __forceinline__ float at(int v) const { return widen(storage, __ldg(c + v)); }
+    __device__ __forceinline__ float3 operator()(int k) const {
+        return make_float3(at(3 * k), at(3 * k + 1), at(3 * k + 2));
+    }
+};
+
 // SH radiance of degree <= 3 (+0.5 bias, clamped at 0) along direction d
-PTIR_DEV float3 sh_radiance(const TraceParams& P, unsigned id, float3 d) {
-    const float* c = P.part.sph + (size_t)id * P.part.sph_stride;
-    float3 rad = ld3(c) * 0.28209479177387814f;
-    const int deg = P.part.sph_degree;
+template <class Coef>
+PTIR_DEV float3 sh_eval(const Coef& c, int deg, float3 d) {
+    float3 rad = c(0) * 0.28209479177387814f;
     if (deg > 0) {
         const float x = d.x, y = d.y, z = d.z;
-        rad = rad - ld3(c + 3) * (0.4886025119029199f * y) + ld3(c + 6) * (0.4886025119029199f * z) -
-              ld3(c + 9) * (0.4886025119029199f * x);
+        rad = rad - c(1) * (0.4886025119029199f * y) + c(2) * (0.4886025119029199f * z) -
+              c(3) * (0.4886025119029199f * x);
         if (deg > 1) {
             const float xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-            rad = rad + ld3(c + 12) * (1.0925484305920792f * xy) + ld3(c + 15) * (-1.0925484305920792f * yz) +
-                  ld3(c + 18) * (0.31539156525252005f * (2.0f * zz - xx - yy)) +
-                  ld3(c + 21) * (-1.0925484305920792f * xz) + ld3(c + 24) * (0.5462742152960396f * (xx - yy));
+            rad = rad + c(4) * (1.0925484305920792f * xy) + c(5) * (-1.0925484305920792f * yz) +
+                  c(6) * (0.31539156525252005f * (2.0f * zz - xx - yy)) +
+                  c(7) * (-1.0925484305920792f * xz) + c(8) * (0.5462742152960396f * (xx - yy));
             if (deg > 2) {
-                rad = rad + ld3(c + 27) * (-0.5900435899266435f * y * (3.0f * xx - yy)) +
-                      ld3(c + 30) * (2.890611442640554f * xy * z) +
-                      ld3(c + 33) * (-0.4570457994644658f * y * (4.0f * zz - xx - yy)) +
-                      ld3(c + 36) * (0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy)) +
-                      ld3(c + 39) * (-0.4570457994644658f * x * (4.0f * zz - xx - yy)) +
-                      ld3(c + 42) * (1.445305721320277f * z * (xx - yy)) +
-                      ld3(c + 45) * (-0.5900435899266435f * x * (xx - 3.0f * yy));
+                rad = rad + c(9) * (-0.5900435899266435f * y * (3.0f * xx - yy)) +
+                      c(10) * (2.890611442640554f * xy * z) +
+                      c(11) * (-0.4570457994644658f * y * (4.0f * zz - xx - yy)) +
+                      c(12) * (0.3731763325901154f * z * (2.0f * zz - 3.0f * xx - 3.0f * yy)) +
+                      c(13) * (-0.4570457994644658f * x * (4.0f * zz - xx - yy)) +
+                      c(14) * (1.445305721320277f * z * (xx - yy)) +
+                      c(15) * (-0.5900435899266435f * x * (xx - 3.0f * yy));
             }
         }
     }
     return relu3(rad + f3(0.5f));
+}
+
+PTIR_DEV float3 sh_radiance(const TraceParams& P, unsigned id, float3 d) {
+    const int deg = P.part.sph_degree;
+    if (P.part.storage == kStoreF32) return sh_eval(ShRowF32{P.part.sph + (size_t)id * P.part.sph_stride}, deg, d);
+    const ShRow16 c{reinterpret_cast<const unsigned short*>(P.part.cold + (size_t)P.part.cold_stride * id + 1),
+                    P.part.storage};
+    return sh_eval(c, deg, d);
 }
 
 // Stochastic shadow transmittance: occluded at the first hit whose alpha beats a draw
@@ -371,80 +394,133 @@ PTIR_DEV void flush_counters(const TraceParams& P, const TraceCounters& c) {
 }
 
 // Front-to-back compositing of one segment over k-buffer batches (pathTracer.cuh:216-311 with
-// processHit, gaussianParticles.cuh:343-440). Accepted Gaussians are flagged in `vis` (when
-// given) as int32 1 inside the float32 tensor, as the reference does (pathTracer.cuh:283-284).
-template <bool kSelfOcc, class Ctx>
-PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
-    const TraceParams& P = C.P;
-    const float2 clip = clip_scene(P, s.o, s.d);
-    const float keep_spdf = s.scatter_pdf, keep_lpdf = s.light_pdf;
-    segment_reset(s, s.o, s.d, fmaxf(0.0f, clip.x - 1e-9f));
-    if (P.flags & kMis) {
-        s.scatter_pdf = keep_spdf;
-        s.light_pdf = keep_lpdf;
-    }
+// processHit, gaussianParticles.cuh:343-440), split so that a schedule can interleave the trace
+// calls of many segments: composite_begin, then while composite_open: one trace call over
+// (composite_tmin, composite_tend), stop if it found nothing, composite_hits; then composite_end.
+constexpr int kMaxRounds = 1 << 16;  // trace calls per segment before the loop-bound error
+
+struct Composite {
+    float3 o, d;
+    float3 radiance, normal, albedo, snrm;
+    float transmittance, depth, hit2, distortion, hits_count, rough, metal;
+    float last_hit, clip_end;
+    bool hit;
+};
+
+PTIR_DEV void composite_begin(const TraceParams& P, Composite& c, float3 o, float3 d) {
+    const float2 clip = clip_scene(P, o, d);
+    c.o = o;
+    c.d = d;
+    c.radiance = c.normal = c.albedo = c.snrm = f3(0.0f);
+    c.transmittance = 1.0f;
+    c.depth = c.hit2 = c.distortion = c.hits_count = c.rough = c.metal = 0.0f;
+    c.last_hit = fmaxf(0.0f, clip.x - 1e-9f);
+    c.clip_end = clip.y;
+    c.hit = false;
+}
+
+PTIR_DEV bool composite_open(const TraceParams& P, const Composite& c) {
+    return c.last_hit <= c.clip_end && c.transmittance > P.min_transmittance;
+}
+PTIR_DEV float composite_tmin(const Composite& c) { return c.last_hit + 1e-9f; }
+PTIR_DEV float composite_tend(const Composite& c) { return c.clip_end + 1e-9f; }
+
+// Composite one k-buffer batch. Accepted Gaussians are flagged in `vis` (when given) as int32 1
+// inside the float32 tensor, as the reference does (pathTracer.cuh:283-284).
+template <bool kSelfOcc, int K>
+PTIR_DEV void composite_hits(const TraceParams& P, TraceCounters& ctr, Composite& c, const float (&kt)[K],
+                             const unsigned (&kid)[K], float* vis) {
     const bool normals = (P.flags & kNormals) != 0;
-    float3 m_alb = f3(0.0f), snrm = f3(0.0f);
-    float m_rgh = 0.0f, m_met = 0.0f;
-    float kt[Ctx::K];
-    unsigned kid[Ctx::K];
-    for (int round = 0; s.last_hit <= clip.y && s.transmittance > P.min_transmittance; ++round) {
-        if (round > (1 << 16)) {
-            atomicOr(P.error_word, kErrLoopBound);
-            break;
-        }
-        trace_kbuf(P.accel, s.o, s.d, s.last_hit + 1e-9f, clip.y + 1e-9f, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
-        if (kid[0] == kNoHit) break;
 #pragma unroll
-        for (int i = 0; i < Ctx::K; ++i) {
-            const unsigned id = kid[i];
-            if (id == kNoHit || !(s.transmittance > P.min_transmittance)) continue;
-            if (kSelfOcc && self_occluded(P, kt[i], id, s.d)) {
-                s.last_hit = fmaxf(s.last_hit, kt[i]);
-                continue;
-            }
-            float dns;
-            const Response r = respond(P, id, s.o, s.d, dns);
-            const bool accept = r.gres > P.min_response && r.alpha > P.alpha_min;
-            if (accept) {
-                ++C.ctr.accepted;
-                const float w = r.alpha * s.transmittance;
-                const float3 grds = r.scl * r.grd * dot(r.grd, -r.gro);
-                const float hit_t = sqrtf(dot(grds, grds));
-                s.radiance += sh_radiance(P, id, s.d) * w;
-                const float* m = P.part.material + 5 * (size_t)id;
-                m_alb += ld3(m) * w;
-                m_rgh += __ldg(m + 3) * w;
-                m_met += __ldg(m + 4) * w;
-                s.transmittance *= (1.0f - r.alpha);
-                s.depth += hit_t * w;
-                s.hit2 += hit_t * hit_t * w;
-                if (normals) {
-                    snrm += ld3(P.part.snrm + 3 * (size_t)id) * w;
-                    const float3 srot = mul_cols(r.rt, r.scl);
-                    s.normal += normalize_or_keep((r.gro + r.grd * (dot(r.grd, -r.gro) - sqrtf(9.0f - r.d2))) * srot) * w;
-                }
-                s.hit = true;
-                const float op = 1.0f - s.transmittance;
-                s.distortion = fmaxf(op * s.hit2 - s.depth * s.depth, 0.0f);
-                if (vis) vis[id] = __int_as_float(1);
-            }
-            s.last_hit = fmaxf(s.last_hit, kt[i]);
-            if (P.flags & kHitCounts) s.hits_count += accept ? 1.0f : 0.0f;
+    for (int i = 0; i < K; ++i) {
+        const unsigned id = kid[i];
+        if (id == kNoHit || !(c.transmittance > P.min_transmittance)) continue;
+        if (kSelfOcc && self_occluded(P, kt[i], id, c.d)) {
+            c.last_hit = fmaxf(c.last_hit, kt[i]);
+            continue;
         }
+        float dns;
+        const Response r = respond(P, id, c.o, c.d, dns);
+        const bool accept = r.gres > P.min_response && r.alpha > P.alpha_min;
+        if (accept) {
+            ++ctr.accepted;
+            const float w = r.alpha * c.transmittance;
+            const float3 grds = r.scl * r.grd * dot(r.grd, -r.gro);
+            const float hit_t = sqrtf(dot(grds, grds));
+            c.radiance += sh_radiance(P, id, c.d) * w;
+            float3 alb;
+            float rgh, met;
+            load_material(P.part, id, alb, rgh, met);
+            c.albedo += alb * w;
+            c.rough += rgh * w;
+            c.metal += met * w;
+            c.transmittance *= (1.0f - r.alpha);
+            c.depth += hit_t * w;
+            c.hit2 += hit_t * hit_t * w;
+            if (normals) {
+                c.snrm += load_snrm(P.part, id) * w;
+                const float3 srot = mul_cols(r.rt, r.scl);
+                c.normal += normalize_or_keep((r.gro + r.grd * (dot(r.grd, -r.gro) - sqrtf(9.0f - r.d2))) * srot) * w;
+            }
+            c.hit = true;
+            const float op = 1.0f - c.transmittance;
+            c.distortion = fmaxf(op * c.hit2 - c.depth * c.depth, 0.0f);
+            if (vis) vis[id] = __int_as_float(1);
+        }
+        c.last_hit = fmaxf(c.last_hit, kt[i]);
+        if (P.flags & kHitCounts) c.hits_count += accept ? 1.0f : 0.0f;
     }
+}
+
+// The segment after compositing: every field reset but the MIS pdfs (kept when MIS is on),
+// the interaction when the segment is opaque enough, else the escape draw.
+PTIR_DEV void composite_end(const TraceParams& P, const Composite& c, float scatter_pdf, float light_pdf, Segment& s,
+                            Pcg32& rng) {
+    segment_reset(s, c.o, c.d, c.last_hit);
+    if (P.flags & kMis) {
+        s.scatter_pdf = scatter_pdf;
+        s.light_pdf = light_pdf;
+    }
+    s.radiance = c.radiance;
+    s.normal = c.normal;
+    s.transmittance = c.transmittance;
+    s.depth = c.depth;
+    s.hit2 = c.hit2;
+    s.distortion = c.distortion;
+    s.hits_count = c.hits_count;
+    s.hit = c.hit;
     const float op = 1.0f - s.transmittance;
     if (s.hit && op > 0.5f) {
         const float inv = 1.0f / fmaxf(op, 1e-12f);
         s.ivalid = true;
         s.pos = s.o + s.d * (s.depth * inv);
-        s.snrm = snrm * inv;
-        s.albedo = m_alb * inv;
-        s.rough = m_rgh * inv;
-        s.metal = m_met * inv;
+        s.snrm = c.snrm * inv;
+        s.albedo = c.albedo * inv;
+        s.rough = c.rough * inv;
+        s.metal = c.metal * inv;
     } else {
         s.escaped = rng.uniform() < s.transmittance;
     }
+}
+
+template <bool kSelfOcc, class Ctx>
+PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
+    const TraceParams& P = C.P;
+    Composite c;
+    composite_begin(P, c, s.o, s.d);
+    float kt[Ctx::K];
+    unsigned kid[Ctx::K];
+    for (int round = 0; composite_open(P, c); ++round) {
+        if (round > kMaxRounds) {
+            atomicOr(P.error_word, kErrLoopBound);
+            break;
+        }
+        trace_kbuf(P.accel, c.o, c.d, composite_tmin(c), composite_tend(c), kt, kid, C.stack, C.stack_t, P.error_word,
+                   C.ctr);
+        if (kid[0] == kNoHit) break;
+        composite_hits<kSelfOcc>(P, C.ctr, c, kt, kid, vis);
+    }
+    composite_end(P, c, s.scatter_pdf, s.light_pdf, s, rng);
 }
 
 // ------------------------------------------------------------------------------------

@@ -5,12 +5,15 @@
 // referenceBwdOptix.cu:27-74). Each warp covers an 8x4 pixel tile so primary rays of a warp
 // are coherent. Candidate gathering is the software LBVH traversal of traverse.cuh.
 #include "path.cuh"
+#include "stages.h"
 
 namespace ptir {
 
+constexpr int kWarpsPerBlock = 4;  // one 8x4 pixel tile per warp
+
 // ------------------------------------------------------------------------------------
 // forward (referenceOptix.cu:27-71)
-__global__ void __launch_bounds__(128) k_trace_fwd(TraceParams P, FwdOutputs O) {
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_fwd(TraceParams P, FwdOutputs O) {
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -73,7 +76,7 @@ __global__ void __launch_bounds__(128) k_trace_fwd(TraceParams P, FwdOutputs O) 
 
 // ------------------------------------------------------------------------------------
 // backward (referenceBwdOptix.cu:27-74)
-__global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_bwd(TraceParams P, BwdInputs B) {
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -120,23 +123,23 @@ __global__ void __launch_bounds__(128) k_trace_bwd(TraceParams P, BwdInputs B) {
     flush_counters(P, ctr);
 }
 
-cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, int block, cudaStream_t s) {
+cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, const StageCtx& sc, cudaStream_t s) {
     const long long tiles = (long long)((p.w + 7) / 8) * ((p.h + 3) / 4) * p.nz;
     if (tiles <= 0) return cudaSuccess;
-    const int warps_per_block = 128 / 32;
-    (void)block;
-    const long long blocks = (tiles + warps_per_block - 1) / warps_per_block;
-    k_trace_fwd<<<(unsigned)blocks, 128, 0, s>>>(p, o);
+    const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    sc.run(kStageMegakernel, p, s, [&](const TraceParams& q) {
+        k_trace_fwd<<<(unsigned)blocks, 32 * kWarpsPerBlock, 0, s>>>(q, o);
+    });
     return cudaGetLastError();
 }
 
-cudaError_t launch_trace_bwd(const TraceParams& p, const BwdInputs& b, int block, cudaStream_t s) {
+cudaError_t launch_trace_bwd(const TraceParams& p, const BwdInputs& b, const StageCtx& sc, cudaStream_t s) {
     const long long tiles = (long long)((p.w + 7) / 8) * ((p.h + 3) / 4) * p.nz;
     if (tiles <= 0) return cudaSuccess;
-    const int warps_per_block = 128 / 32;
-    (void)block;
-    const long long blocks = (tiles + warps_per_block - 1) / warps_per_block;
-    k_trace_bwd<<<(unsigned)blocks, 128, 0, s>>>(p, b);
+    const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    sc.run(kStageMegakernel, p, s, [&](const TraceParams& q) {
+        k_trace_bwd<<<(unsigned)blocks, 32 * kWarpsPerBlock, 0, s>>>(q, b);
+    });
     return cudaGetLastError();
 }
 

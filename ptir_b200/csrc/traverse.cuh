@@ -97,24 +97,45 @@ PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmi
     kbuf_insert(kt, kid, ts, gid);
 }
 
-// Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
-// `stack` holds kStackDepth node indices, `stack_t` their entry distances.
+// A trace call in progress: the next node to visit and the stack depth (the stack itself is
+// the caller's, kStackDepth node indices in `stack` with their entry distances in `stack_t`).
+struct TraceState {
+    float3 inv;
+    float tmin, tend;
+    int node, sp;
+};
+
+// Start a trace call of ray (o, d) over (tmin, tend). Returns true when node visits remain
+// (trace_step), false when (kt, kid) is already final.
 template <int K>
-PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
-                         unsigned (&kid)[K], int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
+PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
+                          unsigned (&kid)[K], TraceState& t, TraceCounters& ctr) {
     kbuf_clear(kt, kid);
     ++ctr.calls;
-    if (A.n <= 0) return;
+    if (A.n <= 0) return false;
     if (A.n == 1) {
         ++ctr.leaves;
         test_leaf(A, 0, o, d, tmin, tend, kt, kid);
         ctr.candidates += kbuf_count(kid);
-        return;
+        return false;
     }
-    const float3 inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-    int sp = 0;
-    int node = 0;
-    while (true) {
+    t.inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    t.tmin = tmin;
+    t.tend = tend;
+    t.node = 0;
+    t.sp = 0;
+    return true;
+}
+
+// One 4-wide node visit of a trace call. Returns false when the call is complete.
+template <int K>
+PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], unsigned (&kid)[K],
+                         int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
+    const float3 inv = t.inv;
+    const float tmin = t.tmin, tend = t.tend;
+    int sp = t.sp;
+    int node = t.node;
+    {
         ++ctr.nodes;
         const float4* nd = A.nodes + 8 * (size_t)node;
         const float4 lx = __ldg(nd + 0), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
@@ -166,7 +187,8 @@ PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, flo
             const int np = __popc(inner);
             if (sp + np > kStackDepth) {
                 atomicOr(err, kErrStackOverflow);
-                break;
+                ctr.candidates += kbuf_count(kid);
+                return false;
             }
             while (inner) {
                 // farthest remaining first
@@ -196,10 +218,26 @@ PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, flo
                     break;
                 }
             }
-            if (!found) break;
+            if (!found) {
+                ctr.candidates += kbuf_count(kid);
+                return false;
+            }
         }
     }
-    ctr.candidates += kbuf_count(kid);
+    t.sp = sp;
+    t.node = node;
+    return true;
+}
+
+// Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
+// `stack` holds kStackDepth node indices, `stack_t` their entry distances.
+template <int K>
+PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
+                         unsigned (&kid)[K], int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
+    TraceState t;
+    if (!trace_start(A, o, d, tmin, tend, kt, kid, t, ctr)) return;
+    while (trace_step(A, o, d, t, kt, kid, stack, stack_t, err, ctr)) {
+    }
 }
 
 }  // namespace ptir

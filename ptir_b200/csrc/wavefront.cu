@@ -2,15 +2,25 @@
 //
 // Paths are processed in chunks of whole 8x4 pixel tiles (slot q of a chunk = lane q % 32 of
 // tile q / 32, so the primary rays of a warp stay coherent). Per chunk, the forward runs
-//   primary  : primary segment, primary outputs, NEE light sample     -> shadow queue | bounce queue
+//   camera   : sampler seed and primary ray of every slot              -> intersect queue
+//   intersect: primary segment                                        (all slots)
+//   primary  : primary outputs, NEE light sample                       -> shadow queue | bounce queue
 //   shadow   : stochastic shadow ray of the NEE sample                -> bounce queue
 //   bounce d : light gathering, path termination, BRDF sample          -> intersect queue
+//   sort     : the intersect queue in (direction octant, origin cell) order
 //   intersect: next segment                                            -> bounce queue
 // and the backward the same with the adjoint stages, whose re-traversals (the reference's
 // rayIntersectBwd) go to a replay queue drained after every bounce stage. Path state lives in
-// HBM between stages; queues are appended with one atomic per warp (ballot + popc). The per-path
-// order of random draws is the megakernel's, so both schedules produce the same paths.
+// HBM between stages; queues are appended with one atomic per warp (ballot + popc). The
+// intersect stage refills lanes one by one (k_wf_trace). The per-path order of random draws is
+// the megakernel's, so both schedules produce the same paths.
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "path.cuh"
 #include "wavefront.h"
@@ -19,7 +29,7 @@ namespace ptir {
 
 namespace {
 
-constexpr int kThreads = 128;
+constexpr int kMaxThreads = 256;  // largest block size; the kernels use warps only, no block barriers
 
 struct WfView {
     Segment* seg;
@@ -107,13 +117,182 @@ PTIR_DEV void write_pbr(const FwdOutputs& O, size_t li, const PathState& ps) {
     CtxT<K> C{P, stack, stack_t, ctr};
 
 // ---------------------------------------------------------------------------------------
+// ray order
+
+// Sort key of a ray: direction octant (3 bits) over the Morton code of its origin's cell, 8 bits
+// per axis of the scene bounds (24 bits). Queue entries past the count get kSortPad, above all.
+constexpr int kSortKeyBits = 28;
+constexpr unsigned kSortPad = 1u << 27;
+
+PTIR_DEV unsigned spread3_8(unsigned v) {
+    v &= 0xFFu;
+    v = (v | (v << 8)) & 0x0000F00Fu;
+    v = (v | (v << 4)) & 0x000C30C3u;
+    v = (v | (v << 2)) & 0x00249249u;
+    return v;
+}
+
+__global__ void __launch_bounds__(kMaxThreads) k_wf_sort_keys(TraceParams P, WfView W, int in_q, unsigned* keys) {
+    const unsigned count = W.count[in_q];
+    float3 lo = f3(0.0f), scale = f3(0.0f);
+    if (P.accel.n > 0) {
+        const float4 a = __ldg(P.accel.bounds), b = __ldg(P.accel.bounds + 1);
+        lo = make_float3(a.x, a.y, a.z);
+        scale = make_float3(255.0f / fmaxf(b.x - a.x, 1e-30f), 255.0f / fmaxf(b.y - a.y, 1e-30f),
+                            255.0f / fmaxf(b.z - a.z, 1e-30f));
+    }
+    for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < W.slots; i += gridDim.x * blockDim.x) {
+        unsigned key = kSortPad;
+        if (i < count) {
+            const unsigned q = W.q[in_q][i];
+            const float3 o = W.seg[q].o, d = W.seg[q].d;
+            const unsigned oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
+            const float3 c = (o - lo) * scale;
+            const unsigned cx = (unsigned)fminf(fmaxf(c.x, 0.0f), 255.0f);
+            const unsigned cy = (unsigned)fminf(fmaxf(c.y, 0.0f), 255.0f);
+            const unsigned cz = (unsigned)fminf(fmaxf(c.z, 0.0f), 255.0f);
+            key = (oct << 24) | (spread3_8(cx) << 2) | (spread3_8(cy) << 1) | spread3_8(cz);
+        }
+        keys[i] = key;
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// intersection with per-lane refill
+
+PTIR_DEV unsigned lanes_below() { return (1u << lane()) - 1u; }
+
+// Intersection stage: each lane carries one segment of queue `in_q` (read from `items`, the
+// queue in queue or sorted order) through as many trace calls as it needs (composite_begin /
+// trace / composite_hits / composite_end). A lane whose call has finished composites its batch
+// and starts the next call, or writes its segment, hands it to queue `out_q` (when >= 0) and
+// takes the next one from the queue, so that no lane waits for the slowest segment of its warp.
+// The warp leaves its traversal loop once `refill` lanes wait (a finished call, or idle while
+// the queue still holds segments).
+template <int K, bool kMark, bool kSelfOcc>
+__global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
+                                                          const unsigned* items, int out_q, unsigned cursor,
+                                                          int refill) {
+    int stack[kStackDepth];
+    float stack_t[kStackDepth];
+    TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    constexpr unsigned kFull = 0xFFFFFFFFu;
+    enum : int { kIdle = 0, kTracing = 1, kReady = 2 };
+    const unsigned count = W.count[in_q];
+    int phase = kIdle;
+    unsigned q = 0;
+    int rounds = 0;
+    bool drained = false;
+    Composite c;
+    TraceState t;
+    float kt[K];
+    unsigned kid[K];
+    // next trace call of this lane's segment, or ready with nothing found when it is complete
+    auto next_call = [&]() {
+        if (!composite_open(P, c)) {
+            kid[0] = kNoHit;
+            phase = kReady;
+            return;
+        }
+        if (++rounds > kMaxRounds + 1) {
+            atomicOr(P.error_word, kErrLoopBound);
+            kid[0] = kNoHit;
+            phase = kReady;
+            return;
+        }
+        phase = trace_start(P.accel, c.o, c.d, composite_tmin(c), composite_tend(c), kt, kid, t, ctr) ? kTracing
+                                                                                                          : kReady;
+    };
+    while (true) {
+        // refill the idle lanes
+        const unsigned idle = __ballot_sync(kFull, phase == kIdle);
+        if (!drained && idle) {
+            const unsigned n_idle = __popc(idle);
+            unsigned base = 0;
+            if (lane() == 0) base = atomicAdd(W.cursor + cursor, n_idle);
+            base = __shfl_sync(kFull, base, 0);
+            drained = base + n_idle >= count;
+            if (phase == kIdle) {
+                const unsigned i = base + __popc(idle & lanes_below());
+                if (i < count) {
+                    q = items[i];
+                    composite_begin(P, c, W.seg[q].o, W.seg[q].d);
+                    ++ctr.segments;
+                    rounds = 0;
+                    next_call();
+                }
+            }
+        }
+        const unsigned busy = __ballot_sync(kFull, phase != kIdle);
+        if (!busy) {
+            if (drained) break;
+            continue;
+        }
+        // traverse until enough lanes wait
+        const unsigned eligible = drained ? busy : kFull;
+        while (true) {
+            const unsigned tracing = __ballot_sync(kFull, phase == kTracing);
+            if (!tracing || __popc(eligible & ~tracing) >= refill) break;
+            if (phase == kTracing &&
+                !trace_step(P.accel, c.o, c.d, t, kt, kid, stack, stack_t, P.error_word, ctr))
+                phase = kReady;
+        }
+        // composite the finished calls; hand on the finished segments
+        bool done = false;
+        if (phase == kReady) {
+            if (kid[0] != kNoHit) {
+                composite_hits<kSelfOcc>(P, ctr, c, kt, kid, kMark ? vis : nullptr);
+                next_call();
+            }
+            // nothing found, segment closed, or loop bound: the segment is complete
+            if (phase == kReady && kid[0] == kNoHit) {
+                Segment s;
+                Pcg32 rng = load_rng(W, q);
+                composite_end(P, c, W.seg[q].scatter_pdf, W.seg[q].light_pdf, s, rng);
+                W.seg[q] = s;
+                store_rng(W, q, rng);
+                phase = kIdle;
+                done = true;
+            }
+        }
+        if (out_q >= 0) push(W.q[out_q], W.count + out_q, q, done);
+    }
+    flush_counters(P, ctr);
+}
+
+// ---------------------------------------------------------------------------------------
 // forward
+
+// Camera segments of the chunk: the sampler seed and the primary ray of every slot inside the
+// image, queued for intersection.
+__global__ void __launch_bounds__(kMaxThreads) k_wf_camera(TraceParams P, WfView W) {
+    while (true) {
+        const unsigned base = fetch32(W.cursor + 0);
+        if (base >= W.slots) break;
+        const unsigned q = base + lane();
+        unsigned x = 0, y = 0, z = 0;
+        const bool valid = q < W.slots && slot_index(P, W, q, x, y, z);
+        if (valid) {
+            Pcg32 rng;
+            rng.seed(x, y, z, P.frame);
+            Segment s;
+            float3 o, d;
+            world_ray(P, launch_of(P, x, y, z), o, d);
+            segment_reset(s, o, d, 0.0f);
+            W.seg[q] = s;
+            store_rng(W, q, rng);
+        }
+        push(W.q[kQIsect], W.count + kQIsect, q, valid);
+    }
+}
+
+// primary outputs and the first NEE sample of every camera segment
 template <int K>
-__global__ void __launch_bounds__(kThreads) k_wf_fwd_primary(TraceParams P, FwdOutputs O, WfView W) {
+__global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_primary(TraceParams P, FwdOutputs O, WfView W) {
     PTIR_STAGE_PROLOGUE
     const bool mis = (P.flags & kMis) != 0;
     while (true) {
-        const unsigned base = fetch32(W.cursor + 0);
+        const unsigned base = fetch32(W.cursor + 2);
         if (base >= W.slots) break;
         const unsigned q = base + lane();
         unsigned x = 0, y = 0, z = 0;
@@ -121,16 +300,10 @@ __global__ void __launch_bounds__(kThreads) k_wf_fwd_primary(TraceParams P, FwdO
         bool cont = false, shadow = false;
         if (valid) {
             const size_t li = launch_of(P, x, y, z);
-            Pcg32 rng;
-            rng.seed(x, y, z, P.frame);
+            Pcg32 rng = load_rng(W, q);
             PathState ps;
             path_init(ps, effective_bounces(P));
-            Segment s;
-            float3 o, d;
-            world_ray(P, li, o, d);
-            segment_reset(s, o, d, 0.0f);
-            ++ctr.segments;
-            intersect_mark<false>(C, s, rng, O.visibility);
+            Segment s = W.seg[q];
             float* r = O.radiance + 3 * li;
             r[0] = s.radiance.x; r[1] = s.radiance.y; r[2] = s.radiance.z;
             O.density[li] = 1.0f - s.transmittance;
@@ -162,11 +335,11 @@ __global__ void __launch_bounds__(kThreads) k_wf_fwd_primary(TraceParams P, FwdO
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads) k_wf_shadow(TraceParams P, WfView W) {
+__global__ void __launch_bounds__(kMaxThreads) k_wf_shadow(TraceParams P, WfView W) {
     PTIR_STAGE_PROLOGUE
     const unsigned count = W.count[kQShadow];
     while (true) {
-        const unsigned base = fetch32(W.cursor + 1);
+        const unsigned base = fetch32(W.cursor + 3);
         if (base >= count) break;
         const unsigned i = base + lane();
         const bool valid = i < count;
@@ -185,7 +358,7 @@ __global__ void __launch_bounds__(kThreads) k_wf_shadow(TraceParams P, WfView W)
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads) k_wf_fwd_bounce(TraceParams P, FwdOutputs O, WfView W, unsigned depth,
+__global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_bounce(TraceParams P, FwdOutputs O, WfView W, unsigned depth,
                                                             unsigned cursor) {
     PTIR_STAGE_PROLOGUE
     const unsigned count = W.count[kQBounce];
@@ -222,37 +395,16 @@ __global__ void __launch_bounds__(kThreads) k_wf_fwd_bounce(TraceParams P, FwdOu
     flush_counters(P, ctr);
 }
 
-template <int K, bool kMark>
-__global__ void __launch_bounds__(kThreads) k_wf_isect(TraceParams P, float* vis, WfView W, unsigned cursor) {
-    PTIR_STAGE_PROLOGUE
-    const unsigned count = W.count[kQIsect];
-    while (true) {
-        const unsigned base = fetch32(W.cursor + cursor);
-        if (base >= count) break;
-        const unsigned i = base + lane();
-        const bool valid = i < count;
-        const unsigned q = valid ? W.q[kQIsect][i] : 0u;
-        if (valid) {
-            Segment s = W.seg[q];
-            Pcg32 rng = load_rng(W, q);
-            ++ctr.segments;
-            intersect_mark<true>(C, s, rng, kMark ? vis : nullptr);
-            W.seg[q] = s;
-            store_rng(W, q, rng);
-        }
-        push(W.q[kQBounce], W.count + kQBounce, q, valid);
-    }
-    flush_counters(P, ctr);
-}
-
 // ---------------------------------------------------------------------------------------
 // backward
+
+// adjoint state and the first NEE sample of every camera segment
 template <int K>
-__global__ void __launch_bounds__(kThreads) k_wb_primary(TraceParams P, BwdInputs B, WfView W) {
+__global__ void __launch_bounds__(kMaxThreads) k_wb_primary(TraceParams P, BwdInputs B, WfView W) {
     PTIR_STAGE_PROLOGUE
     const bool mis = (P.flags & kMis) != 0;
     while (true) {
-        const unsigned base = fetch32(W.cursor + 0);
+        const unsigned base = fetch32(W.cursor + 2);
         if (base >= W.slots) break;
         const unsigned q = base + lane();
         unsigned x = 0, y = 0, z = 0;
@@ -260,20 +412,14 @@ __global__ void __launch_bounds__(kThreads) k_wb_primary(TraceParams P, BwdInput
         bool cont = false, shadow = false;
         if (valid) {
             const size_t li = launch_of(P, x, y, z);
-            Pcg32 rng;
-            rng.seed(x, y, z, P.frame);
+            Pcg32 rng = load_rng(W, q);
             PathState ps;
             path_init(ps, effective_bounces(P));
             ps.acc = ld3(B.pbr + 3 * li);
             ps.acc_grad = B.pbr_grad ? ld3(B.pbr_grad + 3 * li) : f3(0.0f);
             ps.acc_light = ld3(B.light + 3 * li);
             ps.acc_light_grad = B.light_grad ? ld3(B.light_grad + 3 * li) : f3(0.0f);
-            Segment s;
-            float3 o, d;
-            world_ray(P, li, o, d);
-            segment_reset(s, o, d, 0.0f);
-            ++ctr.segments;
-            intersect_mark<false>(C, s, rng, nullptr);
+            Segment s = W.seg[q];
             if (s.ivalid && B.material_grad) {
                 const float* mg = B.material_grad + 5 * li;
                 s.d_albedo += ld3(mg);
@@ -295,7 +441,7 @@ __global__ void __launch_bounds__(kThreads) k_wb_primary(TraceParams P, BwdInput
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads) k_wb_bounce(TraceParams P, BwdInputs B, WfView W, unsigned depth,
+__global__ void __launch_bounds__(kMaxThreads) k_wb_bounce(TraceParams P, BwdInputs B, WfView W, unsigned depth,
                                                         unsigned cursor) {
     PTIR_STAGE_PROLOGUE
     const unsigned count = W.count[kQBounce];
@@ -340,7 +486,7 @@ __global__ void __launch_bounds__(kThreads) k_wb_bounce(TraceParams P, BwdInputs
 }
 
 template <int K>
-__global__ void __launch_bounds__(kThreads) k_wb_replay(TraceParams P, BwdInputs B, WfView W, unsigned cursor) {
+__global__ void __launch_bounds__(kMaxThreads) k_wb_replay(TraceParams P, BwdInputs B, WfView W, unsigned cursor) {
     PTIR_STAGE_PROLOGUE
     const unsigned count = W.count[kQJobs];
     while (true) {
@@ -355,7 +501,8 @@ __global__ void __launch_bounds__(kThreads) k_wb_replay(TraceParams P, BwdInputs
     flush_counters(P, ctr);
 }
 
-int grid_for(const void* fn) {
+// persistent grid: resident blocks per SM x SMs
+int grid_for(const void* fn, int block) {
     static int sms = 0;
     if (sms == 0) {
         int dev = 0;
@@ -364,9 +511,21 @@ int grid_for(const void* fn) {
         if (sms <= 0) sms = 148;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, 0) != cudaSuccess || per_sm <= 0)
-        per_sm = 4;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess || per_sm <= 0)
+        per_sm = 1;
     return sms * per_sm;
+}
+
+// grid of a kernel at a block size, computed once per (kernel, block size)
+int grid_cached(const void* fn, int block) {
+    static std::mutex mu;
+    static std::map<std::pair<const void*, int>, int> cache;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find({fn, block});
+    if (it != cache.end()) return it->second;
+    const int g = grid_for(fn, block);
+    cache[{fn, block}] = g;
+    return g;
 }
 
 }  // namespace
@@ -378,6 +537,7 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
         if (p) cudaFreeAsync(p, s);
     };
     rel(b.seg); rel(b.ps); rel(b.rng); rel(b.q[0]); rel(b.q[1]); rel(b.q[2]); rel(b.jobs);
+    rel(b.sort_keys[0]); rel(b.sort_keys[1]); rel(b.sorted); rel(b.sort_temp);
     void* counters = b.counters;
     b = WavefrontBuffers{};
     b.counters = counters;
@@ -391,12 +551,23 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
     for (int k = 0; k < 3; ++k) get(&b.q[k], sizeof(unsigned) * slots);
     get(&b.jobs, sizeof(ReplayJob) * 2 * slots);
     if (!b.counters) get(&b.counters, sizeof(unsigned) * (kNumQueueCounts + kNumCursors));
+    get(&b.sort_keys[0], sizeof(unsigned) * slots);
+    get(&b.sort_keys[1], sizeof(unsigned) * slots);
+    get(&b.sorted, sizeof(unsigned) * slots);
+    if (e == cudaSuccess) {
+        size_t bytes = 0;
+        e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
+                                            (const unsigned*)nullptr, (unsigned*)nullptr, (int)slots, 0, kSortKeyBits, s);
+        b.sort_temp_bytes = bytes;
+        get(&b.sort_temp, bytes);
+    }
     if (e == cudaSuccess) b.slots = slots;
     return e;
 }
 
 void wavefront_free(WavefrontBuffers& b) {
-    for (void* p : {b.seg, b.ps, b.rng, b.q[0], b.q[1], b.q[2], b.jobs, b.counters})
+    for (void* p : {b.seg, b.ps, b.rng, b.q[0], b.q[1], b.q[2], b.jobs, b.counters, b.sort_keys[0], b.sort_keys[1],
+                    b.sorted, b.sort_temp})
         if (p) cudaFree(p);
     b = WavefrontBuffers{};
 }
@@ -419,38 +590,78 @@ static unsigned long long total_tiles(const TraceParams& p) {
     return (unsigned long long)((p.w + 7) / 8) * ((p.h + 3) / 4) * (unsigned long long)p.nz;
 }
 
+// The intersect queue in ray order (or as queued when sorting is off): keys, then a key/slot
+// radix sort of the whole chunk capacity (the count stays on the device).
+static const unsigned* sort_queue(const TraceParams& p, const WavefrontBuffers& b, const WfView& W,
+                                  const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s) {
+    if (!tune.sort_rays) return W.q[kQIsect];
+    unsigned* keys_in = static_cast<unsigned*>(b.sort_keys[0]);
+    unsigned* keys_out = static_cast<unsigned*>(b.sort_keys[1]);
+    unsigned* sorted = static_cast<unsigned*>(b.sorted);
+    const int grid = grid_cached((const void*)k_wf_sort_keys, tune.block);
+    sc.run(kStageSort, p, s, [&](const TraceParams& q) {
+        k_wf_sort_keys<<<grid, tune.block, 0, s>>>(q, W, kQIsect, keys_in);
+        size_t bytes = b.sort_temp_bytes;
+        cub::DeviceRadixSort::SortPairs(b.sort_temp, bytes, keys_in, keys_out, W.q[kQIsect], sorted, (int)W.slots, 0,
+                                        kSortKeyBits, s);
+    });
+    return sorted;
+}
+
+// Cursor of each stage launch within a chunk: camera 0, primary intersection 1, primary outputs
+// 2, shadow 3, then per bounce depth the bounce stage, (the adjoint's replay,) and intersection.
+constexpr unsigned kFirstBounceCursor = 4;
+
 template <int K>
-static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b, unsigned chunk_tiles,
-                           cudaStream_t s) {
+static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b, const WavefrontTuning& tune,
+                           const StageCtx& sc, cudaStream_t s) {
     const unsigned long long tiles = total_tiles(p);
     if (tiles == 0) return cudaSuccess;
-    chunk_tiles = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles);
+    const unsigned chunk_tiles = (unsigned)std::min<unsigned long long>(tune.chunk_tiles, tiles);
     cudaError_t e = wavefront_reserve(b, (size_t)chunk_tiles * 32, s);
     if (e != cudaSuccess) return e;
-    static int g_primary = 0, g_shadow = 0, g_bounce = 0, g_isect = 0;
-    if (!g_primary) {
-        g_primary = grid_for((const void*)k_wf_fwd_primary<K>);
-        g_shadow = grid_for((const void*)k_wf_shadow<K>);
-        g_bounce = grid_for((const void*)k_wf_fwd_bounce<K>);
-        g_isect = grid_for((const void*)k_wf_isect<K, true>);
-    }
+    const int B = tune.block, R = tune.refill_lanes;
+    const int g_camera = grid_cached((const void*)k_wf_camera, B);
+    const int g_primary = grid_cached((const void*)k_wf_fwd_primary<K>, B);
+    const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
+    const int g_bounce = grid_cached((const void*)k_wf_fwd_bounce<K>, B);
+    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B);
+    const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B);
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
-    if (2u + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
+    if (kFirstBounceCursor + 2u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
         const unsigned nt = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles - t0);
         const WfView W = view_of(b, (unsigned)t0, nt * 32u);
         e = cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * (kNumQueueCounts + kNumCursors), s);
         if (e != cudaSuccess) return e;
-        const int gp = std::min<long long>(g_primary, ((long long)nt * 32 + kThreads - 1) / kThreads);
-        k_wf_fwd_primary<K><<<gp, kThreads, 0, s>>>(p, o, W);
-        if (p.flags & kMis) k_wf_shadow<K><<<g_shadow, kThreads, 0, s>>>(p, W);
-        unsigned cursor = 2;
+        const int cap = (int)std::min<long long>(INT32_MAX, ((long long)nt * 32 + B - 1) / B);
+        sc.run(kStageShading, p, s, [&](const TraceParams& q) {
+            k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
+        });
+        sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
+            k_wf_trace<K, true, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, o.visibility, W, kQIsect,
+                                                                             W.q[kQIsect], -1, 1, R);
+        });
+        sc.run(kStageShading, p, s, [&](const TraceParams& q) {
+            k_wf_fwd_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, o, W);
+        });
+        if (p.flags & kMis)
+            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { k_wf_shadow<K><<<g_shadow, B, 0, s>>>(q, W); });
+        unsigned cursor = kFirstBounceCursor;
         for (unsigned depth = 0; depth < mb; ++depth) {
             cudaMemsetAsync(W.count + kQIsect, 0, sizeof(unsigned), s);
-            k_wf_fwd_bounce<K><<<g_bounce, kThreads, 0, s>>>(p, o, W, depth, cursor++);
+            sc.run(kStageShading, p, s, [&](const TraceParams& q) {
+                k_wf_fwd_bounce<K><<<g_bounce, B, 0, s>>>(q, o, W, depth, cursor);
+            });
+            ++cursor;
             if (depth + 1 >= mb) break;
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
-            k_wf_isect<K, true><<<g_isect, kThreads, 0, s>>>(p, o.visibility, W, cursor++);
+            const unsigned* items = sort_queue(p, b, W, tune, sc, s);
+            sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
+                k_wf_trace<K, true, true><<<g_trace, B, 0, s>>>(q, o.visibility, W, kQIsect, items, kQBounce, cursor,
+                                                                R);
+            });
+            ++cursor;
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -459,40 +670,60 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
 }
 
 template <int K>
-static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontBuffers& b, unsigned chunk_tiles,
-                           cudaStream_t s) {
+static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontBuffers& b, const WavefrontTuning& tune,
+                           const StageCtx& sc, cudaStream_t s) {
     const unsigned long long tiles = total_tiles(p);
     if (tiles == 0) return cudaSuccess;
-    chunk_tiles = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles);
+    const unsigned chunk_tiles = (unsigned)std::min<unsigned long long>(tune.chunk_tiles, tiles);
     cudaError_t e = wavefront_reserve(b, (size_t)chunk_tiles * 32, s);
     if (e != cudaSuccess) return e;
-    static int g_primary = 0, g_shadow = 0, g_bounce = 0, g_isect = 0, g_replay = 0;
-    if (!g_primary) {
-        g_primary = grid_for((const void*)k_wb_primary<K>);
-        g_shadow = grid_for((const void*)k_wf_shadow<K>);
-        g_bounce = grid_for((const void*)k_wb_bounce<K>);
-        g_isect = grid_for((const void*)k_wf_isect<K, false>);
-        g_replay = grid_for((const void*)k_wb_replay<K>);
-    }
+    const int B = tune.block, R = tune.refill_lanes;
+    const int g_camera = grid_cached((const void*)k_wf_camera, B);
+    const int g_primary = grid_cached((const void*)k_wb_primary<K>, B);
+    const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
+    const int g_bounce = grid_cached((const void*)k_wb_bounce<K>, B);
+    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B);
+    const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B);
+    const int g_replay = grid_cached((const void*)k_wb_replay<K>, B);
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
-    if (2u + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
+    if (kFirstBounceCursor + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
         const unsigned nt = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles - t0);
         const WfView W = view_of(b, (unsigned)t0, nt * 32u);
         e = cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * (kNumQueueCounts + kNumCursors), s);
         if (e != cudaSuccess) return e;
-        const int gp = std::min<long long>(g_primary, ((long long)nt * 32 + kThreads - 1) / kThreads);
-        k_wb_primary<K><<<gp, kThreads, 0, s>>>(p, bi, W);
-        if (p.flags & kMis) k_wf_shadow<K><<<g_shadow, kThreads, 0, s>>>(p, W);
-        unsigned cursor = 2;
+        const int cap = (int)std::min<long long>(INT32_MAX, ((long long)nt * 32 + B - 1) / B);
+        sc.run(kStageShading, p, s, [&](const TraceParams& q) {
+            k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
+        });
+        sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
+            k_wf_trace<K, false, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, nullptr, W, kQIsect, W.q[kQIsect],
+                                                                              -1, 1, R);
+        });
+        sc.run(kStageShading, p, s, [&](const TraceParams& q) {
+            k_wb_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, bi, W);
+        });
+        if (p.flags & kMis)
+            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { k_wf_shadow<K><<<g_shadow, B, 0, s>>>(q, W); });
+        unsigned cursor = kFirstBounceCursor;
         for (unsigned depth = 0; depth < mb; ++depth) {
             cudaMemsetAsync(W.count + kQIsect, 0, sizeof(unsigned), s);
             cudaMemsetAsync(W.count + kQJobs, 0, sizeof(unsigned), s);
-            k_wb_bounce<K><<<g_bounce, kThreads, 0, s>>>(p, bi, W, depth, cursor++);
-            k_wb_replay<K><<<g_replay, kThreads, 0, s>>>(p, bi, W, cursor++);
+            sc.run(kStageShading, p, s, [&](const TraceParams& q) {
+                k_wb_bounce<K><<<g_bounce, B, 0, s>>>(q, bi, W, depth, cursor);
+            });
+            ++cursor;
+            sc.run(kStageReplay, p, s, [&](const TraceParams& q) {
+                k_wb_replay<K><<<g_replay, B, 0, s>>>(q, bi, W, cursor);
+            });
+            ++cursor;
             if (depth + 1 >= mb) break;
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
-            k_wf_isect<K, false><<<g_isect, kThreads, 0, s>>>(p, nullptr, W, cursor++);
+            const unsigned* items = sort_queue(p, b, W, tune, sc, s);
+            sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
+                k_wf_trace<K, false, true><<<g_trace, B, 0, s>>>(q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
+            });
+            ++cursor;
         }
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -501,20 +732,20 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
 }
 
 cudaError_t launch_trace_fwd_wavefront(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b,
-                                       unsigned chunk_tiles, int kbuf, cudaStream_t s) {
-    switch (kbuf) {
-    case 8: return run_fwd<8>(p, o, b, chunk_tiles, s);
-    case 32: return run_fwd<32>(p, o, b, chunk_tiles, s);
-    default: return run_fwd<16>(p, o, b, chunk_tiles, s);
+                                       const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s) {
+    switch (tune.kbuf) {
+    case 8: return run_fwd<8>(p, o, b, tune, sc, s);
+    case 32: return run_fwd<32>(p, o, b, tune, sc, s);
+    default: return run_fwd<16>(p, o, b, tune, sc, s);
     }
 }
 
 cudaError_t launch_trace_bwd_wavefront(const TraceParams& p, const BwdInputs& bi, WavefrontBuffers& b,
-                                       unsigned chunk_tiles, int kbuf, cudaStream_t s) {
-    switch (kbuf) {
-    case 8: return run_bwd<8>(p, bi, b, chunk_tiles, s);
-    case 32: return run_bwd<32>(p, bi, b, chunk_tiles, s);
-    default: return run_bwd<16>(p, bi, b, chunk_tiles, s);
+                                       const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s) {
+    switch (tune.kbuf) {
+    case 8: return run_bwd<8>(p, bi, b, tune, sc, s);
+    case 32: return run_bwd<32>(p, bi, b, tune, sc, s);
+    default: return run_bwd<16>(p, bi, b, tune, sc, s);
     }
 }
 

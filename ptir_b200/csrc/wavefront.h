@@ -5,6 +5,7 @@
 #include <stddef.h>
 
 #include "device_types.h"
+#include "stages.h"
 
 namespace ptir {
 
@@ -20,15 +21,28 @@ struct WavefrontBuffers {
     void* q[3] = {nullptr, nullptr, nullptr};  // u32[slots] each
     void* jobs = nullptr;    // ReplayJob[2 * slots]
     void* counters = nullptr;  // u32[kNumQueueCounts + kNumCursors]
+    void* sort_keys[2] = {nullptr, nullptr};  // u32[slots]: ray-order keys, unsorted and sorted
+    void* sorted = nullptr;  // u32[slots]: the intersect queue in key order
+    void* sort_temp = nullptr;
+    size_t sort_temp_bytes = 0;
 };
 
 cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s);
 void wavefront_free(WavefrontBuffers& b);
 
-// chunk_tiles: 8x4 pixel tiles per chunk (32 paths each); kbuf: candidates per traversal (8, 16, 32)
+// Launch shape of the wavefront schedule. Only the k-buffer size can change a result: it moves
+// the distance at which subtrees are culled, which decides which grazing candidate is kept.
+struct WavefrontTuning {
+    unsigned chunk_tiles = 131072;  // 8x4 pixel tiles per chunk (32 paths each)
+    int kbuf = 16;                  // candidates per traversal: 8, 16 or 32
+    int refill_lanes = 32;          // intersection: waiting lanes (1..32) before a warp refills
+    int block = 128;                // threads per block: 64, 128 or 256
+    bool sort_rays = true;          // intersect bounce rays in (direction octant, origin cell) order
+};
+
 cudaError_t launch_trace_fwd_wavefront(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b,
-                                       unsigned chunk_tiles, int kbuf, cudaStream_t s);
+                                       const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s);
 cudaError_t launch_trace_bwd_wavefront(const TraceParams& p, const BwdInputs& bi, WavefrontBuffers& b,
-                                       unsigned chunk_tiles, int kbuf, cudaStream_t s);
+                                       const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s);
 
 }  // namespace ptir

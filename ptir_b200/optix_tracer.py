@@ -35,7 +35,18 @@ def _stream() -> int:
 
 
 class OptixTracer:
-    """Drop-in for ``libthreedgptir_cc.OptixTracer``."""
+    """Drop-in for ``libthreedgptir_cc.OptixTracer``.
+
+    The keyword arguments after the reference's own set the B200 launch shape (no counterpart in
+    the reference): ``schedule`` ("wavefront" or "megakernel"), and for the wavefront
+    ``chunk_tiles`` (8x4 pixel tiles per chunk), ``kbuffer`` (8, 16 or 32 candidates per
+    traversal), ``refill_lanes`` (waiting lanes before an intersection warp refills, 1..32) and
+    ``block_size`` (64, 128 or 256); 0 keeps the default. ``collect_timings`` records CUDA events
+    around every kernel launch for ``stage_times()``; ``sort_rays`` intersects bounce rays in
+    (direction octant, origin cell) order (the results do not change). ``storage`` ("fp32",
+    "bf16" or "fp16") sets how the tracer holds the Gaussians' attributes: in 16-bit storage
+    geometry, material, shading normals and SH are rounded once per call (and by ``build_bvh``)
+    and widened on load, all arithmetic staying FP32."""
 
     def __init__(
         self,
@@ -57,6 +68,11 @@ class OptixTracer:
         schedule: str = "wavefront",
         chunk_tiles: int = 0,
         kbuffer: int = 16,
+        refill_lanes: int = 0,
+        block_size: int = 0,
+        collect_timings: bool = False,
+        sort_rays: bool = True,
+        storage: str = "fp32",
     ):
         if pipeline not in ("reference",):
             raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
@@ -71,7 +87,8 @@ class OptixTracer:
             float(particle_kernel_degree), float(particle_kernel_min_response), int(bool(particle_kernel_density_clamping)),
             self.sph_degree, int(bool(enable_normals)), int(bool(enable_hit_counts)), int(bool(enable_mis)),
             int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
-            N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer))
+            N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
+            int(bool(collect_timings)), 0 if sort_rays else 1, N.STORAGES[storage])
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:
@@ -226,10 +243,23 @@ class OptixTracer:
 
     # --------------------------------------------------------------------------------
     # extensions (not in the reference): counters and device status for tests and benchmarks
-    def counters(self) -> dict:
+    def counters(self, stage: str | None = None) -> dict:
+        """Device counters of the last trace / trace_bwd, of all kernels or of one stage
+        ("intersect", "shadow", "replay", "shading", "megakernel", "sort")."""
         c = N.PtirCounters()
-        N.check(self._h, self._lib.ptir_get_counters(self._h, C.byref(c), _stream()), "counters")
+        if stage is None:
+            rc = self._lib.ptir_get_counters(self._h, C.byref(c), _stream())
+        else:
+            rc = self._lib.ptir_get_stage_counters(self._h, N.STAGES.index(stage), C.byref(c), _stream())
+        N.check(self._h, rc, "counters")
         return c.as_dict()
+
+    def stage_times(self) -> dict:
+        """{stage: (milliseconds, launches)} recorded since the previous call (collect_timings=True):
+        CUDA events around every launch, on the launch stream."""
+        t = N.PtirStageTimes()
+        N.check(self._h, self._lib.ptir_get_stage_times(self._h, C.byref(t)), "stage_times")
+        return {name: (float(t.ms[k]), int(t.launches[k])) for k, name in enumerate(N.STAGES)}
 
     def device_status(self) -> int:
         w = C.c_uint32(0)

@@ -48,12 +48,34 @@ def to_torch(s: dict, device="cuda") -> dict:
 
 
 def make_tracer(sph_degree=3, normals=True, hitcounts=True, mis=True, metallic=False, visualize=False,
-                kernel_degree=4, min_response=0.0113, clamping=True, schedule="wavefront", chunk_tiles=0, kbuffer=16):
+                kernel_degree=4, min_response=0.0113, clamping=True, schedule="wavefront", chunk_tiles=0, kbuffer=16,
+                **launch):
     from ptir_b200 import OptixTracer
 
     return OptixTracer("", "", "reference", "referenceBwd", "instances", kernel_degree, min_response, clamping,
                        sph_degree, normals, hitcounts, mis, metallic, visualize, schedule=schedule,
-                       chunk_tiles=chunk_tiles, kbuffer=kbuffer)
+                       chunk_tiles=chunk_tiles, kbuffer=kbuffer, **launch)
+
+
+def round_to(a: np.ndarray, storage: str) -> np.ndarray:
+    """float32 values rounded to bf16 / fp16 (nearest even) and widened back, as the tracer's
+    16-bit storage holds them."""
+    a = np.ascontiguousarray(a, np.float32)
+    if storage == "fp16":
+        return a.astype(np.float16).astype(np.float32)
+    if storage == "bf16":
+        u = a.view(np.uint32).astype(np.uint64)
+        u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+        return u.astype(np.uint32).view(np.float32)
+    return a
+
+
+ATTRIBUTES = ("build_pos", "build_rot", "build_scl", "build_dns", "density", "material", "sph", "shading_normal")
+
+
+def round_scene(s: dict, storage: str) -> dict:
+    """The scene as a tracer with 16-bit attribute storage sees it."""
+    return dict(s, **{k: round_to(s[k], storage) for k in ATTRIBUTES})
 
 
 def gpu_trace(tr, S: dict, build=True, rebuild=True):
