@@ -1,11 +1,15 @@
 """Benchmark of the Gaussian-field path tracer: forward + adjoint path segments per second.
 
-A step is one inverse-rendering iteration of the tracer on the workload: acceleration-structure
-rebuild, forward trace of every (view, sample) path, L1 loss gradient against a target render,
-and the path-replay adjoint. The default workload is field-1m (1M Gaussians, 8 views of
-1024x768 at 16 spp, 4 bounces, 512x1024 environment; see ptir_b200/synthetic.py).
+A step is one inverse-rendering training iteration on the workload: LBVH refit, forward trace of
+every (view, sample) path, L1 loss gradient against a target render, the path-replay adjoint,
+and the fused selective Adam step of the material and environment. The default workload is
+field-1m (1M Gaussians, 8 views of 1024x768 at 16 spp, 4 bounces, 512x1024 environment; see
+ptir_b200/synthetic.py) with BF16 attribute storage and FP32 arithmetic; --storage fp32 gives
+the plain FP32 drop-in. The metric counts the forward path segments of a step (the adjoint
+replays each of them) over the step's device time.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--impl ours|reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--storage bf16|fp16|fp32]
+                  [--impl ours|reference]
 
 One JSON line on rank 0. Multi-GPU runs (torchrun) are data parallel over views: every rank
 traces its own views of the same scene (weak scaling) and the material / environment
@@ -35,8 +39,10 @@ sys.path.insert(0, ROOT)
 
 from ptir_b200 import dist as pdist  # noqa: E402
 from ptir_b200 import envmap, synthetic  # noqa: E402
+from ptir_b200.optim import selective_adam_  # noqa: E402
 
 METRIC = "fwd+bwd path segments/s at 1M Gaussians"
+ADAM_LR = 1e-3
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 HBM_FALLBACK_GBS = 6650.0
 
@@ -235,13 +241,19 @@ def run_ours(args, rank, world, device):
     del mat_t
     torch.cuda.synchronize()
 
-    def step(ray_ori=None, ray_dir=None, events=None):
-        tr.build_bvh(S.pos, S.rot, S.scl, S.dns, True, True)
+    # optimizer state of the trained attributes: material [N,5] and environment [He,We,4]
+    adam = {k: (torch.zeros_like(t), torch.zeros_like(t)) for k, t in (("material", S.material), ("env", S.env))}
+
+    def step(ray_ori=None, ray_dir=None, events=None, on_fwd=None, on_bwd=None):
+        """One training iteration: LBVH refit, forward, L1 loss gradient, adjoint, selective Adam."""
+        tr.build_bvh(S.pos, S.rot, S.scl, S.dns, False, True)
         if events:
             events[0].record(stream)
         fwd = S.trace(tr, ray_ori=ray_ori, ray_dir=ray_dir)
         if events:
             events[1].record(stream)
+        if on_fwd:
+            on_fwd()
         pbr = fwd[10]
         diff = pbr - target
         loss = diff.abs().mean()
@@ -253,27 +265,28 @@ def run_ours(args, rank, world, device):
         dg, mg, rg, sg, eg = S.trace_bwd(tr, fwd, g, ray_ori=ray_ori, ray_dir=ray_dir)
         if events:
             events[3].record(stream)
+        if on_bwd:
+            on_bwd()
         if world > 1:
             pdist.allreduce_gradients([mg, eg])
+        visible = fwd[9].view(torch.int32) != 0
+        selective_adam_(S.material, mg, *adam["material"], visible, lr=ADAM_LR)
+        selective_adam_(S.env, eg, *adam["env"], None, lr=ADAM_LR)
         return loss
 
     # warm-up (also reads the deterministic per-launch counters, in total and per stage)
-    fc = bc = None
-    fcs, bcs = {}, {}
+    got = {}
+
+    def read(tag):
+        got[tag] = tr.counters()
+        got[tag + "_stages"] = {st: tr.counters(st) for st in STAGES}
+
     for i in range(args.warmup):
-        tr.build_bvh(S.pos, S.rot, S.scl, S.dns, True, True)
-        fwd = S.trace(tr)
         if i == 0:
-            fc = tr.counters()
-            fcs = {st: tr.counters(st) for st in STAGES}
-        if not hasattr(S, "_zeros"):
-            S.prepare_grads(fwd)
-        diff = fwd[10] - target
-        S.trace_bwd(tr, fwd, torch.sign(diff) * (1.0 / diff.numel()))
-        if i == 0:
-            bc = tr.counters()
-            bcs = {st: tr.counters(st) for st in STAGES}
-        del fwd
+            step(on_fwd=lambda: read("fwd"), on_bwd=lambda: read("bwd"))
+        else:
+            step()
+    fc, bc, fcs, bcs = got["fwd"], got["bwd"], got["fwd_stages"], got["bwd_stages"]
     torch.cuda.synchronize()
     status = tr.device_status()
     if status != 0:
@@ -370,7 +383,8 @@ def run_ours(args, rank, world, device):
         "config": {"workload": S.wl.name, "storage": args.storage, "gaussians": S.wl.n, "views_per_gpu": len(S.wl.views), "resolution": [w, h],
                    "spp": spp, "max_bounces": S.wl.max_bounces, "env": list(S.wl.env_hw),
                    "samples_per_gpu": S.samples, "segments_per_step_per_gpu": segs,
-                   "step": "bvh rebuild + forward + L1 loss grad + adjoint" + (" + grad all-reduce" if world > 1 else ""),
+                   "step": "lbvh refit + forward + L1 loss grad + adjoint + selective adam (material, env)"
+                           + (" + grad all-reduce" if world > 1 else ""),
                    "l2": "inputs larger than L2 (scene + BVH records ~400 MB)", "parallelism": f"dp{world} over views"},
         "pass_ms": {"forward": fwd_ms, "backward": bwd_ms},
         "stages_ms_per_step": {KERNEL_OF_STAGE[st]: stage_t[st][0] / args.steps for st in STAGES if stage_t[st][1]},
@@ -444,7 +458,7 @@ def main():
     ap.add_argument("--res", default=None, help="WxH")
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--storage", default="fp32", choices=("fp32", "bf16", "fp16"),
+    ap.add_argument("--storage", default="bf16", choices=("fp32", "bf16", "fp16"),
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

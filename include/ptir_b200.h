@@ -213,6 +213,14 @@ int ptir_scene_bounds(ptir_tracer* tracer, float* out6, void* stream);
  * leaves [N*16] floats (see ptir_b200/csrc/device_types.h for the record layouts); synchronises. */
 int ptir_debug_accel(ptir_tracer* tracer, float* nodes_host, float* leaves_host, void* stream);
 
+/* Fused selective Adam step of the training iteration (SelectiveAdam.step,
+ * threedgrut/optimizers/__init__.py:89-125 and optimizers.cu:49-76): param, grad, exp_avg and
+ * exp_avg_sq are [n_rows, row] float32 device arrays; rows whose visible[r] is 0 are skipped
+ * (visible may be null: every row). No bias correction, as in the reference. Asynchronous on
+ * `stream`; needs no tracer. */
+int ptir_selective_adam(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, const uint8_t* visible,
+                        int64_t n_rows, int32_t row, float lr, float beta1, float beta2, float eps, void* stream);
+
 const char* ptir_last_error(const ptir_tracer* tracer);
 
 /* Allocation-free scene bounds. This entry point has no counterpart in the reference.

@@ -102,7 +102,7 @@ class PtirCounters(C.Structure):
 
 EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", "ptir_trace", "ptir_trace_bwd",
            "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_device_status",
-           "ptir_scene_bounds", "ptir_debug_accel", "ptir_last_error")
+           "ptir_scene_bounds", "ptir_debug_accel", "ptir_selective_adam", "ptir_last_error")
 
 
 def lib_path() -> str:
@@ -144,6 +144,9 @@ def load(build_if_missing: bool = True):
     L.ptir_scene_bounds.restype = C.c_int
     L.ptir_debug_accel.argtypes = [C.c_void_p, _FP, _FP, C.c_void_p]
     L.ptir_debug_accel.restype = C.c_int
+    L.ptir_selective_adam.argtypes = [_FP, _FP, _FP, _FP, _FP, C.c_int64, C.c_int32, C.c_float, C.c_float, C.c_float,
+                                      C.c_float, C.c_void_p]
+    L.ptir_selective_adam.restype = C.c_int
     L.ptir_last_error.argtypes = [C.c_void_p]
     L.ptir_last_error.restype = C.c_char_p
     _LIB = L

@@ -220,10 +220,15 @@ class Tracer:
         enable_metallic = _conf_get(r, "enable_metallic", None)
         if enable_metallic is None:
             enable_metallic = _conf_get(_conf_get(conf, "model"), "optimize_material_metallic", False)
+        # B200 launch shape and attribute storage (render.b200.*; absent keys keep the defaults)
+        b2 = _conf_get(r, "b200")
+        launch = {k: _conf_get(b2, k) for k in ("schedule", "chunk_tiles", "kbuffer", "refill_lanes", "block_size",
+                                                 "sort_rays", "storage")}
         self.tracer_wrapper = OptixTracer(
             "", "", r.pipeline_type, r.backward_pipeline_type, r.primitive_type, r.particle_kernel_degree,
             r.particle_kernel_min_response, r.particle_kernel_density_clamping, r.particle_radiance_sph_degree,
-            r.enable_normals, r.enable_hitcounts, r.enable_mis, bool(enable_metallic), self.visualize_lights)
+            r.enable_normals, r.enable_hitcounts, r.enable_mis, bool(enable_metallic), self.visualize_lights,
+            **{k: v for k, v in launch.items() if v is not None})
         self.frame_timer = _EventTimer() if _conf_get(r, "enable_kernel_timings", False) else None
         self.timings = {}
 
