@@ -194,6 +194,25 @@ int ptir_trace(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_trac
 int ptir_trace_bwd(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_bwd_args* bwd,
                    const ptir_bwd_outputs* out, void* stream);
 
+/* One camera view of a batched trace. No counterpart in the reference, whose launches share one
+ * extent: a batch traces views of different resolutions and sample counts in one launch
+ * sequence, each exactly as its own ptir_trace would (same per-path seeds, same outputs). */
+typedef struct ptir_view {
+    int32_t z, h, w;             /* launch extent of the view (Z = spp x cameras) */
+    uint32_t frame;              /* frameNumber of the view */
+    const float* ray_to_world;   /* [>=1,4,4] of the view; only the first matrix applies */
+} ptir_view;
+
+#define PTIR_MAX_VIEWS 64
+
+/* trace / trace_bwd over `nviews` (1..PTIR_MAX_VIEWS) views: ray_origin, ray_direction and every
+ * per-sample input and output are the views' [Z,H,W,C] arrays concatenated in view order (flat,
+ * sum of Z*H*W rows); the args' own z, h, w, frame and ray_to_world are ignored. */
+int ptir_trace_views(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_view* views, int32_t nviews,
+                     const ptir_trace_outputs* out, void* stream);
+int ptir_trace_bwd_views(ptir_tracer* tracer, const ptir_trace_args* args, const ptir_view* views, int32_t nviews,
+                         const ptir_bwd_args* bwd, const ptir_bwd_outputs* out, void* stream);
+
 /* Counters of the last launch; synchronises `stream`. */
 int ptir_get_counters(ptir_tracer* tracer, ptir_counters* out, void* stream);
 

@@ -47,6 +47,13 @@ STORAGES = {"fp32": 0, "bf16": 1, "fp16": 2}
 STAGES = ("intersect", "shadow", "replay", "shading", "megakernel", "sort")
 
 
+class PtirView(C.Structure):
+    _fields_ = [("z", C.c_int32), ("h", C.c_int32), ("w", C.c_int32), ("frame", C.c_uint32), ("ray_to_world", _FP)]
+
+
+MAX_VIEWS = 64
+
+
 class PtirStageTimes(C.Structure):
     _fields_ = [("ms", C.c_double * len(STAGES)), ("launches", C.c_uint64 * len(STAGES))]
 
@@ -101,7 +108,7 @@ class PtirCounters(C.Structure):
 
 
 EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", "ptir_trace", "ptir_trace_bwd",
-           "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_device_status",
+           "ptir_trace_views", "ptir_trace_bwd_views", "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_device_status",
            "ptir_scene_bounds", "ptir_debug_accel", "ptir_selective_adam", "ptir_last_error")
 
 
@@ -132,6 +139,12 @@ def load(build_if_missing: bool = True):
     L.ptir_trace.restype = C.c_int
     L.ptir_trace_bwd.argtypes = [C.c_void_p, P(PtirTraceArgs), P(PtirBwdArgs), P(PtirBwdOutputs), C.c_void_p]
     L.ptir_trace_bwd.restype = C.c_int
+    L.ptir_trace_views.argtypes = [C.c_void_p, P(PtirTraceArgs), P(PtirView), C.c_int32, P(PtirTraceOutputs),
+                                   C.c_void_p]
+    L.ptir_trace_views.restype = C.c_int
+    L.ptir_trace_bwd_views.argtypes = [C.c_void_p, P(PtirTraceArgs), P(PtirView), C.c_int32, P(PtirBwdArgs),
+                                       P(PtirBwdOutputs), C.c_void_p]
+    L.ptir_trace_bwd_views.restype = C.c_int
     L.ptir_get_counters.argtypes = [C.c_void_p, P(PtirCounters), C.c_void_p]
     L.ptir_get_counters.restype = C.c_int
     L.ptir_get_stage_counters.argtypes = [C.c_void_p, C.c_int32, P(PtirCounters), C.c_void_p]

@@ -11,6 +11,8 @@
 #include "storage.cuh"
 #include "wavefront.h"
 
+static_assert(PTIR_MAX_VIEWS == ptir::kMaxViews, "view table size of the C ABI");
+static_assert(sizeof(ptir::TraceParams) <= 4000, "kernel parameters must stay within 4 KB");
 static_assert((int)PTIR_STAGE_INTERSECT == (int)ptir::kStageIntersect &&
                   (int)PTIR_STAGE_SHADOW == (int)ptir::kStageShadow &&
                   (int)PTIR_STAGE_REPLAY == (int)ptir::kStageReplay &&
@@ -75,13 +77,36 @@ unsigned flags_of(const ptir_config& c) {
 }
 
 // checks shared by trace and trace_bwd; fills the kernel parameters
-int prepare(ptir_tracer* t, const ptir_trace_args* a, ptir::TraceParams& p) {
+// checks shared by every trace entry point; fills the kernel parameters and the launch count.
+// `views` null: the single launch of the reference (args' extent, frame and ray_to_world).
+int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, int nviews, ptir::TraceParams& p,
+            long long& launches) {
     if (!a) return fail(t, PTIR_EINVAL, "null trace arguments");
-    if (a->z < 0 || a->h < 0 || a->w < 0) return fail(t, PTIR_EINVAL, "negative launch extent");
-    const long long launches = (long long)a->z * a->h * a->w;
-    if (launches > 0 && (!a->ray_origin || !a->ray_direction || !a->ray_to_world))
-        return fail(t, PTIR_EINVAL, "ray_origin, ray_direction and ray_to_world are required");
-    if (launches > (1ll << 31) - 1) return fail(t, PTIR_EINVAL, "launch extent exceeds 2^31 - 1 paths");
+    ptir_view single;
+    if (!views) {
+        single.z = a->z;
+        single.h = a->h;
+        single.w = a->w;
+        single.frame = a->frame;
+        single.ray_to_world = a->ray_to_world;
+        views = &single;
+        nviews = 1;
+    }
+    if (nviews < 1 || nviews > PTIR_MAX_VIEWS)
+        return fail(t, PTIR_EINVAL, "view count must lie in [1, " + std::to_string(PTIR_MAX_VIEWS) + "]");
+    launches = 0;
+    long long tiles = 0;
+    for (int v = 0; v < nviews; ++v) {
+        const ptir_view& V = views[v];
+        if (V.z < 0 || V.h < 0 || V.w < 0) return fail(t, PTIR_EINVAL, "negative launch extent");
+        const long long n = (long long)V.z * V.h * V.w;
+        if (n > 0 && !V.ray_to_world) return fail(t, PTIR_EINVAL, "ray_to_world is required");
+        launches += n;
+        tiles += (long long)((V.w + 7) / 8) * ((V.h + 3) / 4) * V.z;
+        if (launches > (1ll << 31) - 1) return fail(t, PTIR_EINVAL, "launch extent exceeds 2^31 - 1 paths");
+    }
+    if (launches > 0 && (!a->ray_origin || !a->ray_direction))
+        return fail(t, PTIR_EINVAL, "ray_origin and ray_direction are required");
     if (a->max_bounces > 64) return fail(t, PTIR_EINVAL, "max_bounces above 64");
     if (!t->accel.valid) return fail(t, PTIR_ESTATE, "trace called before build_bvh");
     if (a->n != t->accel.n)
@@ -128,13 +153,24 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, ptir::TraceParams& p) {
     p.env.cos_z = (float)std::cos((double)rot_z);
     p.env.sin_x = 0.0f;
     p.env.cos_x = 1.0f;
-    p.ray_to_world = a->ray_to_world;
     p.ray_ori = a->ray_origin;
     p.ray_dir = a->ray_direction;
-    p.nz = a->z;
-    p.h = a->h;
-    p.w = a->w;
-    p.frame = a->frame;
+    long long offset = 0, tile0 = 0;
+    for (int v = 0; v < nviews; ++v) {
+        const ptir_view& V = views[v];
+        ptir::ViewDesc& D = p.views[v];
+        D.offset = offset;
+        D.tile0 = tile0;
+        D.to_world = V.ray_to_world;
+        D.w = V.w;
+        D.h = V.h;
+        D.z = V.z;
+        D.frame = V.frame;
+        offset += (long long)V.z * V.h * V.w;
+        tile0 += (long long)((V.w + 7) / 8) * ((V.h + 3) / 4) * V.z;
+    }
+    p.nviews = nviews;
+    p.tiles = tiles;
     p.flags = flags_of(t->cfg);
     p.kernel_degree = (int)t->cfg.kernel_degree;
     p.min_response = t->cfg.kernel_min_response;
@@ -262,13 +298,18 @@ int ptir_build_bvh(ptir_tracer* t, const float* pos, const float* rot, const flo
     return PTIR_OK;
 }
 
-int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_outputs* o, void* stream) {
+}  // extern "C"
+
+namespace {
+
+int trace_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, int nviews,
+               const ptir_trace_outputs* o, void* stream) {
     if (!t) return PTIR_EINVAL;
     ptir::TraceParams p;
-    const int rc = prepare(t, a, p);
+    long long launches = 0;
+    const int rc = prepare(t, a, views, nviews, p, launches);
     if (rc != PTIR_OK) return rc;
     if (!o) return fail(t, PTIR_EINVAL, "null outputs");
-    const long long launches = (long long)a->z * a->h * a->w;
     if (launches > 0 && (!o->radiance || !o->density || !o->hit_distance || !o->hit_distance_second_moment ||
                          !o->depth_distortion || !o->normal || !o->shading_normal || !o->material || !o->hits_count ||
                          !o->pbr || !o->light || !o->pbr_components))
@@ -306,14 +347,14 @@ int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_output
     return PTIR_OK;
 }
 
-int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args* b, const ptir_bwd_outputs* o,
-                   void* stream) {
+int trace_bwd_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, int nviews,
+                   const ptir_bwd_args* b, const ptir_bwd_outputs* o, void* stream) {
     if (!t) return PTIR_EINVAL;
     ptir::TraceParams p;
-    const int rc = prepare(t, a, p);
+    long long launches = 0;
+    const int rc = prepare(t, a, views, nviews, p, launches);
     if (rc != PTIR_OK) return rc;
     if (!b || !o) return fail(t, PTIR_EINVAL, "null backward arguments");
-    const long long launches = (long long)a->z * a->h * a->w;
     if (launches > 0 && (!b->pbr || !b->light)) return fail(t, PTIR_EINVAL, "forward pbr and light are required");
     if (a->n > 0 && !o->particle_material_grad) return fail(t, PTIR_EINVAL, "particle_material_grad is required");
     cudaStream_t s = as_stream(stream);
@@ -346,6 +387,31 @@ int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args
             : ptir::launch_trace_bwd_wavefront(p, bi, t->wave, tuning_of(t->cfg), sc, s);
     if (e != cudaSuccess) return cuda_fail(t, e, "trace_bwd launch");
     return PTIR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ptir_trace(ptir_tracer* t, const ptir_trace_args* a, const ptir_trace_outputs* o, void* stream) {
+    return trace_impl(t, a, nullptr, 0, o, stream);
+}
+
+int ptir_trace_bwd(ptir_tracer* t, const ptir_trace_args* a, const ptir_bwd_args* b, const ptir_bwd_outputs* o,
+                   void* stream) {
+    return trace_bwd_impl(t, a, nullptr, 0, b, o, stream);
+}
+
+int ptir_trace_views(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, int32_t nviews,
+                     const ptir_trace_outputs* o, void* stream) {
+    if (!views) return fail(t, PTIR_EINVAL, "null view table");
+    return trace_impl(t, a, views, nviews, o, stream);
+}
+
+int ptir_trace_bwd_views(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, int32_t nviews,
+                         const ptir_bwd_args* b, const ptir_bwd_outputs* o, void* stream) {
+    if (!views) return fail(t, PTIR_EINVAL, "null view table");
+    return trace_bwd_impl(t, a, views, nviews, b, o, stream);
 }
 
 int ptir_get_counters(ptir_tracer* t, ptir_counters* out, void* stream) {

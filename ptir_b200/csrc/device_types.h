@@ -57,15 +57,29 @@ struct ParticleView {
     int cold_stride;         // uint4 per cold record
 };
 
+// One launch of a batch (a camera view with its own extent and sample count). Launch indices
+// of a view run over (z, y, x) row-major from `offset` in the batch's flat ray and output arrays;
+// its 8x4 pixel tiles run from `tile0` in the batch's tile order. Paths are seeded from the
+// view's own (x, y, z) and frame, so a batch traces exactly what separate launches would.
+struct ViewDesc {
+    long long offset;
+    long long tile0;
+    const float* to_world;  // [4, 4] row-major (only the first matrix of a launch applies)
+    int w, h, z;
+    unsigned frame;
+};
+
+constexpr int kMaxViews = 64;  // views of one batch (passed by value with the kernel parameters)
+
 struct TraceParams {
     AccelView accel;
     ParticleView part;
     EnvView env;
-    const float* ray_to_world;   // [>=1, 4, 4] row-major; the first matrix applies to every ray
     const float* ray_ori;        // [z, h, w, 3]
     const float* ray_dir;
-    int nz, h, w;
-    unsigned frame;
+    ViewDesc views[kMaxViews];   // the launches of this trace (one for the reference's single launch)
+    int nviews;
+    long long tiles;             // 8x4 pixel tiles of all views
     unsigned flags;
     int kernel_degree;
     float min_response;          // hitMinGaussianResponse

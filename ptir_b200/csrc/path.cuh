@@ -356,8 +356,8 @@ PTIR_DEV void path_init(PathState& ps, unsigned max_bounces) {
     ps.pend_bounces = 0u;
 }
 
-PTIR_DEV void world_ray(const TraceParams& P, size_t li, float3& o, float3& d) {
-    const float* m = P.ray_to_world;
+PTIR_DEV void world_ray(const TraceParams& P, int view, size_t li, float3& o, float3& d) {
+    const float* m = P.views[view].to_world;
     const float3 lo = ld3(P.ray_ori + 3 * li), ld = ld3(P.ray_dir + 3 * li);
     const float3 m0 = ld3(m), m1 = ld3(m + 4), m2 = ld3(m + 8);
     o = make_float3(dot(m0, lo) + __ldg(m + 3), dot(m1, lo) + __ldg(m + 7), dot(m2, lo) + __ldg(m + 11));
@@ -368,18 +368,31 @@ PTIR_DEV unsigned effective_bounces(const TraceParams& P) {
     return P.render_opts ? min(P.max_bounces, 2u) : P.max_bounces;
 }
 
-// launch index of this thread: warps own 8x4 pixel tiles, tiles row-major, then z
-PTIR_DEV bool launch_index(const TraceParams& P, unsigned& x, unsigned& y, unsigned& z) {
-    const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned tiles_x = (unsigned)(P.w + 7) >> 3, tiles_y = (unsigned)(P.h + 3) >> 2;
-    const unsigned per_z = tiles_x * tiles_y;
-    z = warp / per_z;
-    const unsigned t = warp - z * per_z;
+// Lane `lane` of 8x4 pixel tile `tile` of the batch: its view, launch index (x, y, z) within the
+// view and flat launch index li; false past the last tile or outside the view's image.
+PTIR_DEV bool tile_launch(const TraceParams& P, long long tile, unsigned lane, int& view, unsigned& x, unsigned& y,
+                          unsigned& z, size_t& li) {
+    if (tile < 0 || tile >= P.tiles) return false;
+    int v = 0;
+    while (v + 1 < P.nviews && P.views[v + 1].tile0 <= tile) ++v;
+    const ViewDesc& V = P.views[v];
+    const unsigned tiles_x = (unsigned)(V.w + 7) >> 3, tiles_y = (unsigned)(V.h + 3) >> 2;
+    const unsigned long long local = (unsigned long long)(tile - V.tile0);
+    const unsigned long long per_z = (unsigned long long)tiles_x * tiles_y;
+    z = (unsigned)(local / per_z);
+    const unsigned t = (unsigned)(local - (unsigned long long)z * per_z);
     const unsigned ty = t / tiles_x, tx = t - ty * tiles_x;
     x = (tx << 3) + (lane & 7u);
     y = (ty << 2) + (lane >> 3);
-    return z < (unsigned)P.nz && x < (unsigned)P.w && y < (unsigned)P.h;
+    view = v;
+    li = (size_t)V.offset + ((size_t)z * V.h + y) * V.w + x;
+    return z < (unsigned)V.z && x < (unsigned)V.w && y < (unsigned)V.h;
+}
+
+// launch index of this thread in the megakernel: warps own 8x4 pixel tiles
+PTIR_DEV bool launch_index(const TraceParams& P, int& view, unsigned& x, unsigned& y, unsigned& z, size_t& li) {
+    const long long warp = (long long)((blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x) >> 5);
+    return tile_launch(P, warp, threadIdx.x & 31u, view, x, y, z, li);
 }
 
 PTIR_DEV void flush_counters(const TraceParams& P, const TraceCounters& c) {

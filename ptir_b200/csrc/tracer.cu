@@ -19,15 +19,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_fwd(TraceParams P
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     CtxT<kKBuf> C{P, stack, stack_t, ctr};
     unsigned x, y, z;
-    if (launch_index(P, x, y, z)) {
-        const size_t li = ((size_t)z * P.h + y) * P.w + x;
+    int view;
+    size_t li;
+    if (launch_index(P, view, x, y, z, li)) {
         Pcg32 rng;
-        rng.seed(x, y, z, P.frame);
+        rng.seed(x, y, z, P.views[view].frame);
         PathState ps;
         path_init(ps, effective_bounces(P));
         Segment s;
         float3 o, d;
-        world_ray(P, li, o, d);
+        world_ray(P, view, li, o, d);
         segment_reset(s, o, d, 0.0f);
         ++ctr.segments;
         intersect_mark<false>(C, s, rng, O.visibility);
@@ -82,10 +83,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_bwd(TraceParams P
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     CtxT<kKBuf> C{P, stack, stack_t, ctr};
     unsigned x, y, z;
-    if (launch_index(P, x, y, z)) {
-        const size_t li = ((size_t)z * P.h + y) * P.w + x;
+    int view;
+    size_t li;
+    if (launch_index(P, view, x, y, z, li)) {
         Pcg32 rng;
-        rng.seed(x, y, z, P.frame);
+        rng.seed(x, y, z, P.views[view].frame);
         PathState ps;
         path_init(ps, effective_bounces(P));
         ps.acc = ld3(B.pbr + 3 * li);
@@ -94,7 +96,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_bwd(TraceParams P
         ps.acc_light_grad = B.light_grad ? ld3(B.light_grad + 3 * li) : f3(0.0f);
         Segment s;
         float3 o, d;
-        world_ray(P, li, o, d);
+        world_ray(P, view, li, o, d);
         segment_reset(s, o, d, 0.0f);
         ++ctr.segments;
         intersect_mark<false>(C, s, rng, nullptr);
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_bwd(TraceParams P
 }
 
 cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, const StageCtx& sc, cudaStream_t s) {
-    const long long tiles = (long long)((p.w + 7) / 8) * ((p.h + 3) / 4) * p.nz;
+    const long long tiles = p.tiles;
     if (tiles <= 0) return cudaSuccess;
     const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
     sc.run(kStageMegakernel, p, s, [&](const TraceParams& q) {
@@ -134,7 +136,7 @@ cudaError_t launch_trace_fwd(const TraceParams& p, const FwdOutputs& o, const St
 }
 
 cudaError_t launch_trace_bwd(const TraceParams& p, const BwdInputs& b, const StageCtx& sc, cudaStream_t s) {
-    const long long tiles = (long long)((p.w + 7) / 8) * ((p.h + 3) / 4) * p.nz;
+    const long long tiles = p.tiles;
     if (tiles <= 0) return cudaSuccess;
     const long long blocks = (tiles + kWarpsPerBlock - 1) / kWarpsPerBlock;
     sc.run(kStageMegakernel, p, s, [&](const TraceParams& q) {

@@ -39,7 +39,7 @@ struct WfView {
     unsigned* count;         // [kNumQueueCounts]
     unsigned* cursor;        // [kNumCursors]
     ReplayJob* jobs;
-    unsigned tile0;          // first tile of the chunk
+    unsigned long long tile0;  // first tile of the chunk
     unsigned slots;          // paths in the chunk (32 per tile)
 };
 
@@ -75,21 +75,11 @@ PTIR_DEV void push_job(ReplayJob* jobs, unsigned* count, const ReplayJob& j, boo
     if (pred) jobs[base + __popc(mask & ((1u << lane()) - 1u))] = j;
 }
 
-// slot q of the chunk -> launch index (x, y, z); false for slots outside the image
-PTIR_DEV bool slot_index(const TraceParams& P, const WfView& W, unsigned q, unsigned& x, unsigned& y, unsigned& z) {
-    const unsigned tile = W.tile0 + (q >> 5), ln = q & 31u;
-    const unsigned tiles_x = (unsigned)(P.w + 7) >> 3, tiles_y = (unsigned)(P.h + 3) >> 2;
-    const unsigned per_z = tiles_x * tiles_y;
-    z = tile / per_z;
-    const unsigned t = tile - z * per_z;
-    const unsigned ty = t / tiles_x, tx = t - ty * tiles_x;
-    x = (tx << 3) + (ln & 7u);
-    y = (ty << 2) + (ln >> 3);
-    return z < (unsigned)P.nz && x < (unsigned)P.w && y < (unsigned)P.h;
-}
-
-PTIR_DEV size_t launch_of(const TraceParams& P, unsigned x, unsigned y, unsigned z) {
-    return ((size_t)z * P.h + y) * P.w + x;
+// slot q of the chunk -> view, launch index (x, y, z) and flat launch index li; false for slots
+// outside every image
+PTIR_DEV bool slot_index(const TraceParams& P, const WfView& W, unsigned q, int& view, unsigned& x, unsigned& y,
+                         unsigned& z, size_t& li) {
+    return tile_launch(P, (long long)W.tile0 + (q >> 5), q & 31u, view, x, y, z, li);
 }
 
 PTIR_DEV void store_rng(const WfView& W, unsigned q, const Pcg32& r) { W.rng[q] = r.state; }
@@ -271,13 +261,15 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_camera(TraceParams P, WfView
         if (base >= W.slots) break;
         const unsigned q = base + lane();
         unsigned x = 0, y = 0, z = 0;
-        const bool valid = q < W.slots && slot_index(P, W, q, x, y, z);
+        int view = 0;
+        size_t li = 0;
+        const bool valid = q < W.slots && slot_index(P, W, q, view, x, y, z, li);
         if (valid) {
             Pcg32 rng;
-            rng.seed(x, y, z, P.frame);
+            rng.seed(x, y, z, P.views[view].frame);
             Segment s;
             float3 o, d;
-            world_ray(P, launch_of(P, x, y, z), o, d);
+            world_ray(P, view, li, o, d);
             segment_reset(s, o, d, 0.0f);
             W.seg[q] = s;
             store_rng(W, q, rng);
@@ -296,10 +288,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_primary(TraceParams P, F
         if (base >= W.slots) break;
         const unsigned q = base + lane();
         unsigned x = 0, y = 0, z = 0;
-        const bool valid = q < W.slots && slot_index(P, W, q, x, y, z);
+        int view = 0;
+        size_t li = 0;
+        const bool valid = q < W.slots && slot_index(P, W, q, view, x, y, z, li);
         bool cont = false, shadow = false;
         if (valid) {
-            const size_t li = launch_of(P, x, y, z);
             Pcg32 rng = load_rng(W, q);
             PathState ps;
             path_init(ps, effective_bounces(P));
@@ -386,8 +379,10 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_bounce(TraceParams P, Fw
                 store_rng(W, q, rng);
             } else {
                 unsigned x, y, z;
-                slot_index(P, W, q, x, y, z);
-                write_pbr(O, launch_of(P, x, y, z), ps);
+                int view;
+                size_t li;
+                slot_index(P, W, q, view, x, y, z, li);
+                write_pbr(O, li, ps);
             }
         }
         push(W.q[kQIsect], W.count + kQIsect, q, cont);
@@ -408,10 +403,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_wb_primary(TraceParams P, BwdIn
         if (base >= W.slots) break;
         const unsigned q = base + lane();
         unsigned x = 0, y = 0, z = 0;
-        const bool valid = q < W.slots && slot_index(P, W, q, x, y, z);
+        int view = 0;
+        size_t li = 0;
+        const bool valid = q < W.slots && slot_index(P, W, q, view, x, y, z, li);
         bool cont = false, shadow = false;
         if (valid) {
-            const size_t li = launch_of(P, x, y, z);
             Pcg32 rng = load_rng(W, q);
             PathState ps;
             path_init(ps, effective_bounces(P));
@@ -572,7 +568,7 @@ void wavefront_free(WavefrontBuffers& b) {
     b = WavefrontBuffers{};
 }
 
-static WfView view_of(const WavefrontBuffers& b, unsigned tile0, unsigned slots) {
+static WfView view_of(const WavefrontBuffers& b, unsigned long long tile0, unsigned slots) {
     WfView W;
     W.seg = static_cast<Segment*>(b.seg);
     W.ps = static_cast<PathState*>(b.ps);
@@ -586,9 +582,7 @@ static WfView view_of(const WavefrontBuffers& b, unsigned tile0, unsigned slots)
     return W;
 }
 
-static unsigned long long total_tiles(const TraceParams& p) {
-    return (unsigned long long)((p.w + 7) / 8) * ((p.h + 3) / 4) * (unsigned long long)p.nz;
-}
+static unsigned long long total_tiles(const TraceParams& p) { return (unsigned long long)p.tiles; }
 
 // The intersect queue in ray order (or as queued when sorting is off): keys, then a key/slot
 // radix sort of the whole chunk capacity (the count stays on the device).
@@ -631,7 +625,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
     if (kFirstBounceCursor + 2u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
         const unsigned nt = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles - t0);
-        const WfView W = view_of(b, (unsigned)t0, nt * 32u);
+        const WfView W = view_of(b, t0, nt * 32u);
         e = cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * (kNumQueueCounts + kNumCursors), s);
         if (e != cudaSuccess) return e;
         const int cap = (int)std::min<long long>(INT32_MAX, ((long long)nt * 32 + B - 1) / B);
@@ -689,7 +683,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
     if (kFirstBounceCursor + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
         const unsigned nt = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles - t0);
-        const WfView W = view_of(b, (unsigned)t0, nt * 32u);
+        const WfView W = view_of(b, t0, nt * 32u);
         e = cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * (kNumQueueCounts + kNumCursors), s);
         if (e != cudaSuccess) return e;
         const int cap = (int)std::min<long long>(INT32_MAX, ((long long)nt * 32 + B - 1) / B);

@@ -34,6 +34,16 @@ def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
 
+def split_views(flat: torch.Tensor, views) -> list:
+    """Per-view [Z,H,W,C...] views of a flat per-sample tensor [T,C...] of trace_views()."""
+    out, start = [], 0
+    for _, _, z, h, w in views:
+        n = int(z) * int(h) * int(w)
+        out.append(flat[start:start + n].reshape(int(z), int(h), int(w), *flat.shape[1:]))
+        start += n
+    return out
+
+
 class OptixTracer:
     """Drop-in for ``libthreedgptir_cc.OptixTracer``.
 
@@ -173,7 +183,7 @@ class OptixTracer:
     def trace(self, frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material, particle_radiance,
               particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
               mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table, sh_indirect,
-              sph_degree, min_transmittance, max_bounces):
+              sph_degree, min_transmittance, max_bounces, _views=None):
         """trace (optixTracer.cpp:909-1013). Returns (rayRad, rayDns, rayHit[...,2], rayHitSecondMoment,
         rayDepthDistortion, rayNrm, rayShadingNrm, rayMaterial, rayHitsCount, particleVisibility, rayPbr,
         rayLight, rayPbrComponents)."""
@@ -193,7 +203,10 @@ class OptixTracer:
             _ptr(out["radiance"]), _ptr(out["density"]), _ptr(out["hit"]), _ptr(out["hit2"]), _ptr(out["distortion"]),
             _ptr(out["normal"]), _ptr(out["snormal"]), _ptr(out["material"]), _ptr(out["hits"]), _ptr(pbr),
             _ptr(light), _ptr(comps), _ptr(vis))
-        rc = self._lib.ptir_trace(self._h, C.byref(a), C.byref(o), _stream())
+        if _views is None:
+            rc = self._lib.ptir_trace(self._h, C.byref(a), C.byref(o), _stream())
+        else:
+            rc = self._lib.ptir_trace_views(self._h, C.byref(a), _views, len(_views), C.byref(o), _stream())
         N.check(self._h, rc, "trace")
         del keep
         return (out["radiance"], out["density"], out["hit"], out["hit2"], out["distortion"], out["normal"],
@@ -205,7 +218,7 @@ class OptixTracer:
                   lights, light_alias_table, mesh_light_vertices, mesh_light_triangles, mesh_lights,
                   mesh_light_triangle_alias_table, ray_rad_grd, ray_dns_grd, ray_hit_grd, ray_hit_second_moment_grd,
                   ray_depth_distortion_grd, ray_nrm_grd, ray_shading_nrm_grd, ray_material_grd, ray_pbr_grd,
-                  ray_light_grd, sh_indirect, sph_degree, min_transmittance, max_bounces):
+                  ray_light_grd, sh_indirect, sph_degree, min_transmittance, max_bounces, _views=None):
         """traceBwd (optixTracer.cpp:1015-1145). Returns (densityGrad [N,12], materialGrad [N,5],
         radianceGrad [N,C], shadingNormalGrad [N,3], environmentGrad like environment); as in the
         reference only the material and environment gradients are non-zero."""
@@ -236,10 +249,77 @@ class OptixTracer:
         env_grad = torch.zeros_like(environment)
         b = N.PtirBwdArgs(_ptr(pbr), _ptr(light), _ptr(pbr_g), _ptr(light_g), _ptr(mat_g))
         o = N.PtirBwdOutputs(_ptr(material_grad), _ptr(env_grad) if env is not None else None)
-        rc = self._lib.ptir_trace_bwd(self._h, C.byref(a), C.byref(b), C.byref(o), _stream())
+        if _views is None:
+            rc = self._lib.ptir_trace_bwd(self._h, C.byref(a), C.byref(b), C.byref(o), _stream())
+        else:
+            rc = self._lib.ptir_trace_bwd_views(self._h, C.byref(a), _views, len(_views), C.byref(b), C.byref(o),
+                                                _stream())
         N.check(self._h, rc, "trace_bwd")
         del keep
         return density_grad, material_grad, radiance_grad, snrm_grad, env_grad
+
+    # --------------------------------------------------------------------------------
+    # batched views (not in the reference): several views of their own extent in one launch sequence
+    def _view_table(self, views):
+        """views: sequence of (frame, ray_to_world [>=1,4,4], z, h, w). Returns the C table, the
+        tensors to keep alive, and the total launch count."""
+        if not 1 <= len(views) <= N.MAX_VIEWS:
+            raise ValueError(f"between 1 and {N.MAX_VIEWS} views per batch")
+        table = (N.PtirView * len(views))()
+        keep, total = [], 0
+        for k, (frame, t2w, z, h, w) in enumerate(views):
+            t2w = _f32(t2w, "ray_to_world")
+            if t2w.numel() < 12:
+                raise ValueError("ray_to_world must hold at least one 3x4 (or 4x4) transform")
+            keep.append(t2w)
+            table[k] = N.PtirView(int(z), int(h), int(w), int(frame) & 0xFFFFFFFF, _ptr(t2w))
+            total += int(z) * int(h) * int(w)
+        return table, keep, total
+
+    def trace_views(self, views, ray_ori, ray_dir, particle_density, particle_material, particle_radiance,
+                    particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
+                    mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table,
+                    sh_indirect, sph_degree, min_transmittance, max_bounces):
+        """trace() over a batch of views of their own extent and sample count, in one launch
+        sequence. `views` lists (frame, ray_to_world, z, h, w); ray_ori / ray_dir are the views'
+        [Z,H,W,3] rays concatenated in view order, [T,3]. Returns the 13 outputs of trace() with
+        every per-sample output flat, [T,C] (split_views() cuts them per view); each view's
+        values are those of its own trace() call."""
+        table, keep_t, total = self._view_table(views)
+        ori, dirs = _f32(ray_ori, "ray_ori").reshape(1, 1, -1, 3), _f32(ray_dir, "ray_dir").reshape(1, 1, -1, 3)
+        if ori.shape[2] != total or dirs.shape != ori.shape:
+            raise ValueError(f"ray_ori / ray_dir must hold the {total} rays of the views")
+        out = self.trace(views[0][0], keep_t[0], ori, dirs, particle_density, particle_material, particle_radiance,
+                         particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
+                         mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table,
+                         sh_indirect, sph_degree, min_transmittance, max_bounces, _views=table)
+        flat = [t if k == 9 else t.reshape(total, *t.shape[3:]) for k, t in enumerate(out)]
+        del keep_t
+        return tuple(flat)
+
+    def trace_bwd_views(self, views, ray_ori, ray_dir, ray_rad, ray_dns, ray_hit, ray_hit_second_moment,
+                        ray_depth_distortion, ray_nrm, ray_shading_nrm, ray_material, ray_pbr, ray_light,
+                        particle_density, particle_material, particle_radiance, particle_shading_normal, environment,
+                        environment_alias_table, lights, light_alias_table, mesh_light_vertices, mesh_light_triangles,
+                        mesh_lights, mesh_light_triangle_alias_table, ray_rad_grd, ray_dns_grd, ray_hit_grd,
+                        ray_hit_second_moment_grd, ray_depth_distortion_grd, ray_nrm_grd, ray_shading_nrm_grd,
+                        ray_material_grd, ray_pbr_grd, ray_light_grd, sh_indirect, sph_degree, min_transmittance,
+                        max_bounces):
+        """trace_bwd() over a batch of views; per-sample inputs flat [T,C] as trace_views() returns them."""
+        table, keep_t, total = self._view_table(views)
+        r = lambda t: None if t is None else t.reshape(1, 1, total, -1)  # noqa: E731
+        ori, dirs = r(_f32(ray_ori, "ray_ori")), r(_f32(ray_dir, "ray_dir"))
+        res = self.trace_bwd(views[0][0], keep_t[0], ori, dirs, r(ray_rad), r(ray_dns), r(ray_hit),
+                             r(ray_hit_second_moment), r(ray_depth_distortion), r(ray_nrm), r(ray_shading_nrm),
+                             r(ray_material), r(ray_pbr), r(ray_light), particle_density, particle_material,
+                             particle_radiance, particle_shading_normal, environment, environment_alias_table, lights,
+                             light_alias_table, mesh_light_vertices, mesh_light_triangles, mesh_lights,
+                             mesh_light_triangle_alias_table, r(ray_rad_grd), r(ray_dns_grd), r(ray_hit_grd),
+                             r(ray_hit_second_moment_grd), r(ray_depth_distortion_grd), r(ray_nrm_grd),
+                             r(ray_shading_nrm_grd), r(ray_material_grd), r(ray_pbr_grd), r(ray_light_grd),
+                             sh_indirect, sph_degree, min_transmittance, max_bounces, _views=table)
+        del keep_t
+        return res
 
     # --------------------------------------------------------------------------------
     # extensions (not in the reference): counters and device status for tests and benchmarks
