@@ -59,8 +59,11 @@ def _peaks():
 # ------------------------------------------------------------------------------------------
 # workload setup
 def workload_of(args):
-    """The named workload, optionally shrunk for profiling (--views/--res/--spp)."""
+    """The named workload, optionally shrunk for profiling (--views/--res/--spp; these make every
+    view alike)."""
     wl = synthetic.workload(args.workload)
+    if not any(getattr(args, k, None) for k in ("res", "spp", "views")):
+        return wl
     w, h, spp = wl.views[0]
     if getattr(args, "res", None):
         w, h = (int(v) for v in args.res.lower().split("x"))
@@ -85,24 +88,34 @@ class Setup:
         env = synthetic.make_environment(*wl.env_hw, seed=wl.seed)
         self.env = d(env)
         self.alias = envmap.pack(envmap.build(env), device)
-        # rays of every view and sample: launch z = sample * views + view (the reference's order);
         # with W ranks the job has W x views views and this rank traces its shard
         world = int(os.environ.get("WORLD_SIZE", "1"))
         all_eyes = synthetic.camera_positions(len(wl.views) * world, seed=wl.seed)
         eyes = all_eyes[list(pdist.shard(len(all_eyes), rank, world))]
-        w, h, spp = wl.views[0]
-        assert all(v == wl.views[0] for v in wl.views), "bench workloads use one resolution per launch"
-        oris, dirs = [], []
-        for v, eye in enumerate(eyes):
-            o, dr = synthetic.view_rays_device(w, h, spp, eye, device)
-            oris.append(o)
-            dirs.append(dr)
-        self.ray_ori = torch.stack(oris, 1).reshape(spp * len(eyes), h, w, 3).contiguous()
-        self.ray_dir = torch.stack(dirs, 1).reshape(spp * len(eyes), h, w, 3).contiguous()
-        del oris, dirs
         self.t2w = torch.eye(4, device=device).reshape(1, 4, 4).contiguous()
-        self.samples = int(self.ray_ori.shape[0] * h * w)
-        self.shape = (int(self.ray_ori.shape[0]), h, w)
+        self.batched = any(v != wl.views[0] for v in wl.views)
+        oris, dirs = [], []
+        if not self.batched:
+            # one launch: z = sample * views + view (the reference's order)
+            w, h, spp = wl.views[0]
+            for eye in eyes:
+                o, dr = synthetic.view_rays_device(w, h, spp, eye, device)
+                oris.append(o)
+                dirs.append(dr)
+            self.ray_ori = torch.stack(oris, 1).reshape(spp * len(eyes), h, w, 3).contiguous()
+            self.ray_dir = torch.stack(dirs, 1).reshape(spp * len(eyes), h, w, 3).contiguous()
+        else:
+            # views of their own resolution and spp, one batch: rays flat in view order
+            self.views = []
+            for v, ((w, h, spp), eye) in enumerate(zip(wl.views, eyes)):
+                o, dr = synthetic.view_rays_device(w, h, spp, eye, device)
+                oris.append(o.reshape(-1, 3))
+                dirs.append(dr.reshape(-1, 3))
+                self.views.append((v, self.t2w, spp, h, w))
+            self.ray_ori = torch.cat(oris).contiguous()
+            self.ray_dir = torch.cat(dirs).contiguous()
+        del oris, dirs
+        self.samples = int(self.ray_ori.numel() // 3)
         e = lambda *s, dt=torch.float32: torch.empty(s, dtype=dt, device=device)  # noqa: E731
         self.lights = (e(0, 9), e(5, 0), e(0, 3), e(0, 3, dt=torch.int32), e(0, 8), e(3, 0))
 
@@ -113,19 +126,26 @@ class Setup:
                            False, False, **kw)
 
     def trace(self, tr, material=None, ray_ori=None, ray_dir=None, frame=0):
-        return tr.trace(frame, self.t2w, self.ray_ori if ray_ori is None else ray_ori,
-                        self.ray_dir if ray_dir is None else ray_dir, self.density,
-                        self.material if material is None else material, self.sph, self.snrm, self.env, self.alias,
-                        *self.lights, 0, 3, 0.001, self.wl.max_bounces)
+        ori = self.ray_ori if ray_ori is None else ray_ori
+        drs = self.ray_dir if ray_dir is None else ray_dir
+        mat = self.material if material is None else material
+        scene = (self.density, mat, self.sph, self.snrm, self.env, self.alias, *self.lights, 0, 3, 0.001,
+                 self.wl.max_bounces)
+        if self.batched:
+            return tr.trace_views(self.views, ori, drs, *scene)
+        return tr.trace(frame, self.t2w, ori, drs, *scene)
 
     def trace_bwd(self, tr, fwd, pbr_grad, ray_ori=None, ray_dir=None, frame=0):
         (rad, dns, hit, hit2, dist, nrm, snrm, mat, hits, vis, pbr, light, comps) = fwd
         z = self._zeros
-        return tr.trace_bwd(frame, self.t2w, self.ray_ori if ray_ori is None else ray_ori,
-                            self.ray_dir if ray_dir is None else ray_dir, rad, dns, hit, hit2, dist, nrm, snrm, mat, pbr,
-                            light, self.density, self.material, self.sph, self.snrm, self.env, self.alias, *self.lights,
-                            z["rad"], z["dns"], z["hit"], z["hit2"], z["dist"], z["nrm"], z["snrm"], z["mat"], pbr_grad,
-                            z["light"], 0, 3, 0.001, self.wl.max_bounces)
+        ori = self.ray_ori if ray_ori is None else ray_ori
+        drs = self.ray_dir if ray_dir is None else ray_dir
+        args = (rad, dns, hit, hit2, dist, nrm, snrm, mat, pbr, light, self.density, self.material, self.sph, self.snrm,
+                self.env, self.alias, *self.lights, z["rad"], z["dns"], z["hit"], z["hit2"], z["dist"], z["nrm"],
+                z["snrm"], z["mat"], pbr_grad, z["light"], 0, 3, 0.001, self.wl.max_bounces)
+        if self.batched:
+            return tr.trace_bwd_views(self.views, ori, drs, *args)
+        return tr.trace_bwd(frame, self.t2w, ori, drs, *args)
 
     def prepare_grads(self, fwd):
         (rad, dns, hit, hit2, dist, nrm, snrm, mat, hits, vis, pbr, light, comps) = fwd
@@ -226,6 +246,12 @@ def algorithmic_bytes(fc: dict, bc: dict, samples: int):
     return fwd, bwd
 
 
+def _view_config(views):
+    if all(v == views[0] for v in views):
+        return {"resolution": list(views[0][:2]), "spp": views[0][2]}
+    return {"views": [list(v) for v in views]}
+
+
 def run_ours(args, rank, world, device):
     import torch.distributed as dist
 
@@ -292,12 +318,36 @@ def run_ours(args, rank, world, device):
     if status != 0:
         raise RuntimeError(f"device loop bound hit during warm-up (status {status})")
 
+    # the step's ray inputs: device buffers refilled from pinned host memory in the e2e loop
+    ori_d, dir_d = S.ray_ori.clone(), S.ray_dir.clone()
+    graph, stage_t, stage_steps = None, None, args.steps
+    if args.graph:
+        if world > 1:
+            raise SystemExit("--graph runs on one GPU")
+        # stage times of one eager step (no events can be recorded inside the graph), then the
+        # whole iteration is captured once and replayed
+        tr.stage_times()
+        step(ray_ori=ori_d, ray_dir=dir_d)
+        torch.cuda.synchronize()
+        stage_t, stage_steps = tr.stage_times(), 1
+        tr.set_collect_timings(False)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            step(ray_ori=ori_d, ray_dir=dir_d)
+        torch.cuda.current_stream().wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            graph_loss = step(ray_ori=ori_d, ray_dir=dir_d)
+        torch.cuda.synchronize()
+
     # timed region, inputs resident in HBM
     clock_lines, stop = [], threading.Event()
     sampler = threading.Thread(target=_clock_sampler, args=(clock_lines, stop, torch.cuda.current_device()), daemon=True)
     sampler.start()
     time.sleep(0.3)
-    tr.stage_times()  # forget the warm-up launches
+    if graph is None:
+        tr.stage_times()  # forget the warm-up launches
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
@@ -305,7 +355,10 @@ def run_ours(args, rank, world, device):
     torch.cuda.synchronize()
     t0.record(stream)
     for k in range(args.steps):
-        step(events=ev[k])
+        if graph is not None:
+            graph.replay()
+        else:
+            step(events=ev[k])
     t1.record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -313,14 +366,16 @@ def run_ours(args, rank, world, device):
     stop.set()
     sampler.join(timeout=10)
     ms_total = t0.elapsed_time(t1)
-    stage_t = tr.stage_times()  # {stage: (ms, launches)} over the timed steps
-    fwd_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
-    bwd_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
+    if graph is None:
+        stage_t = tr.stage_times()  # {stage: (ms, launches)} over the timed steps
+        fwd_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+        bwd_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
+    else:
+        fwd_ms = bwd_ms = None
 
     # end to end through the public API with host buffers: rays H2D each step, loss D2H
     ori_h = S.ray_ori.cpu().pin_memory()
     dir_h = S.ray_dir.cpu().pin_memory()
-    ori_d, dir_d = torch.empty_like(S.ray_ori), torch.empty_like(S.ray_dir)
     e_steps = 1
     if world > 1:
         dist.barrier()
@@ -330,12 +385,17 @@ def run_ours(args, rank, world, device):
     for _ in range(e_steps):
         ori_d.copy_(ori_h, non_blocking=True)
         dir_d.copy_(dir_h, non_blocking=True)
-        loss = step(ray_ori=ori_d, ray_dir=dir_d)
+        if graph is not None:
+            graph.replay()
+            loss = graph_loss
+        else:
+            loss = step(ray_ori=ori_d, ray_dir=dir_d)
         loss_h = loss.to("cpu", non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / e_steps
     _ = float(loss_h)
+    del graph
 
     status = tr.device_status()
     if status != 0:
@@ -360,13 +420,12 @@ def run_ours(args, rank, world, device):
     dom_ms_total, dom_launches = stage_t[dom]
     rec = record_bytes(args.storage)
     dom_bytes_step = stage_bytes(dom, fcs[dom], rec) + stage_bytes(dom, bcs[dom], rec)
-    launches_step = dom_launches / args.steps
+    launches_step = dom_launches / stage_steps
     dom_bytes = dom_bytes_step / launches_step
     dom_ms = dom_ms_total / dom_launches
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
-    w, h, spp = S.wl.views[0]
-    launches_per_step = ACCEL_KERNELS_PER_BUILD + sum(n for _, n in stage_t.values()) / args.steps
+    launches_per_step = ACCEL_KERNELS_PER_BUILD + sum(n for _, n in stage_t.values()) / stage_steps
     res = {
         "metric": METRIC,
         "value": total_segs / (ms_step * 1e-3),
@@ -380,14 +439,15 @@ def run_ours(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": S.wl.name, "storage": args.storage, "gaussians": S.wl.n, "views_per_gpu": len(S.wl.views), "resolution": [w, h],
-                   "spp": spp, "max_bounces": S.wl.max_bounces, "env": list(S.wl.env_hw),
+        "config": {"workload": S.wl.name, "storage": args.storage, "gaussians": S.wl.n,
+                   "views_per_gpu": len(S.wl.views), **_view_config(S.wl.views),
+                   "max_bounces": S.wl.max_bounces, "env": list(S.wl.env_hw), "cuda_graph": bool(args.graph),
                    "samples_per_gpu": S.samples, "segments_per_step_per_gpu": segs,
                    "step": "lbvh refit + forward + L1 loss grad + adjoint + selective adam (material, env)"
                            + (" + grad all-reduce" if world > 1 else ""),
                    "l2": "inputs larger than L2 (scene + BVH records ~400 MB)", "parallelism": f"dp{world} over views"},
         "pass_ms": {"forward": fwd_ms, "backward": bwd_ms},
-        "stages_ms_per_step": {KERNEL_OF_STAGE[st]: stage_t[st][0] / args.steps for st in STAGES if stage_t[st][1]},
+        "stages_ms_per_step": {KERNEL_OF_STAGE[st]: stage_t[st][0] / stage_steps for st in STAGES if stage_t[st][1]},
         "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom], "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
                      "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
@@ -458,6 +518,7 @@ def main():
     ap.add_argument("--res", default=None, help="WxH")
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--graph", action="store_true", help="capture the training iteration in a CUDA graph")
     ap.add_argument("--storage", default="bf16", choices=("fp32", "bf16", "fp16"),
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -479,8 +540,8 @@ def main():
             "impl": "reference", "metric": METRIC, "value": v, "unit": "segments/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl.name, "gaussians": wl.n, "views_per_gpu": len(wl.views), "resolution": [w, h],
-                       "spp": spp, "max_bounces": wl.max_bounces},
+            "config": {"workload": wl.name, "gaussians": wl.n, "views_per_gpu": len(wl.views),
+                       **_view_config(wl.views), "max_bounces": wl.max_bounces},
             "cpu_baseline": {"value": v, "unit": "segments/s", "cores": base["cores"], "kind": "port",
                              "sample": base["sample"]},
             "e2e": {"value": v, "unit": "segments/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -222,6 +222,9 @@ int ptir_get_stage_counters(ptir_tracer* tracer, int32_t stage, ptir_counters* o
 /* Stage times recorded since the previous call, then cleared; waits for the recorded events. */
 int ptir_get_stage_times(ptir_tracer* tracer, ptir_stage_times* out);
 
+/* Turn the launch timing of collect_timings on or off (off while a CUDA graph is captured). */
+int ptir_set_collect_timings(ptir_tracer* tracer, int32_t on);
+
 /* Bounded-loop status word of the last launches (0 = clean); synchronises `stream` and clears it. */
 int ptir_device_status(ptir_tracer* tracer, uint32_t* status_word, void* stream);
 

@@ -108,7 +108,7 @@ class PtirCounters(C.Structure):
 
 
 EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", "ptir_trace", "ptir_trace_bwd",
-           "ptir_trace_views", "ptir_trace_bwd_views", "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_device_status",
+           "ptir_trace_views", "ptir_trace_bwd_views", "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_set_collect_timings", "ptir_device_status",
            "ptir_scene_bounds", "ptir_debug_accel", "ptir_selective_adam", "ptir_last_error")
 
 
@@ -151,6 +151,8 @@ def load(build_if_missing: bool = True):
     L.ptir_get_stage_counters.restype = C.c_int
     L.ptir_get_stage_times.argtypes = [C.c_void_p, P(PtirStageTimes)]
     L.ptir_get_stage_times.restype = C.c_int
+    L.ptir_set_collect_timings.argtypes = [C.c_void_p, C.c_int32]
+    L.ptir_set_collect_timings.restype = C.c_int
     L.ptir_device_status.argtypes = [C.c_void_p, P(C.c_uint32), C.c_void_p]
     L.ptir_device_status.restype = C.c_int
     L.ptir_scene_bounds.argtypes = [C.c_void_p, P(C.c_float), C.c_void_p]

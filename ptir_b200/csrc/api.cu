@@ -424,6 +424,12 @@ int ptir_get_stage_counters(ptir_tracer* t, int32_t stage, ptir_counters* out, v
     return read_counters(t, stage, stage + 1, out, stream);
 }
 
+int ptir_set_collect_timings(ptir_tracer* t, int32_t on) {
+    if (!t) return PTIR_EINVAL;
+    t->timer.enabled = on != 0;
+    return PTIR_OK;
+}
+
 int ptir_get_stage_times(ptir_tracer* t, ptir_stage_times* out) {
     if (!t || !out) return PTIR_EINVAL;
     double ms[ptir::kNumStages] = {};

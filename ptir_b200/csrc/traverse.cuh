@@ -71,6 +71,18 @@ PTIR_DEV void slab(float3 lo, float3 hi, float3 o, float3 inv, float& t0, float&
     t1 = fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz));
 }
 
+// three-input minimum / maximum (one instruction on sm_100a); a NaN input is ignored
+PTIR_DEV float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+PTIR_DEV float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // exact instance test of leaf record p
 template <int K>
 PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
@@ -138,19 +150,25 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
     {
         ++ctr.nodes;
         const float4* nd = A.nodes + 8 * (size_t)node;
-        const float4 lx = __ldg(nd + 0), ly = __ldg(nd + 1), lz = __ldg(nd + 2);
-        const float4 hx = __ldg(nd + 3), hy = __ldg(nd + 4), hz = __ldg(nd + 5), cc = __ldg(nd + 6);
-        const float lxa[4] = {lx.x, lx.y, lx.z, lx.w}, lya[4] = {ly.x, ly.y, ly.z, ly.w}, lza[4] = {lz.x, lz.y, lz.z, lz.w};
-        const float hxa[4] = {hx.x, hx.y, hx.z, hx.w}, hya[4] = {hy.x, hy.y, hy.z, hy.w}, hza[4] = {hz.x, hz.y, hz.z, hz.w};
+        // near and far plane rows of each axis from the direction's signs (rows: lo.x lo.y lo.z
+        // hi.x hi.y hi.z), so each slab interval needs no min / max of its two plane distances
+        const int rx = inv.x >= 0.0f ? 0 : 3, ry = inv.y >= 0.0f ? 1 : 4, rz = inv.z >= 0.0f ? 2 : 5;
+        const float4 nx = __ldg(nd + rx), ny = __ldg(nd + ry), nz = __ldg(nd + rz);
+        const float4 fx = __ldg(nd + (3 - rx)), fy = __ldg(nd + (5 - ry)), fz = __ldg(nd + (7 - rz));
+        const float4 cc = __ldg(nd + 6);
+        const float nxa[4] = {nx.x, nx.y, nx.z, nx.w}, nya[4] = {ny.x, ny.y, ny.z, ny.w};
+        const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fxa[4] = {fx.x, fx.y, fx.z, fx.w};
+        const float fya[4] = {fy.x, fy.y, fy.z, fy.w}, fza[4] = {fz.x, fz.y, fz.z, fz.w};
         const int ch[4] = {__float_as_int(cc.x), __float_as_int(cc.y), __float_as_int(cc.z), __float_as_int(cc.w)};
         float t0[4], key[4];
         bool hit[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            float a, b;
-            slab(make_float3(lxa[k], lya[k], lza[k]), make_float3(hxa[k], hya[k], hza[k]), o, inv, a, b);
-            a = fmaxf(a, tmin);
-            b = fminf(b, tend);
+            // clipped slab interval [a, b]; a NaN plane distance (0 * inf) leaves its axis unbounded
+            const float a =
+                max3f((nxa[k] - o.x) * inv.x, (nya[k] - o.y) * inv.y, fmaxf((nza[k] - o.z) * inv.z, tmin));
+            const float b =
+                min3f((fxa[k] - o.x) * inv.x, (fya[k] - o.y) * inv.y, fminf((fza[k] - o.z) * inv.z, tend));
             t0[k] = a;
             // nearer middle of the clipped interval first: boxes that contain the origin all
             // enter at tmin, their extent along the ray tells them apart

@@ -334,6 +334,10 @@ class OptixTracer:
         N.check(self._h, rc, "counters")
         return c.as_dict()
 
+    def set_collect_timings(self, on: bool) -> None:
+        """Launch timing on or off (keep it off while capturing a CUDA graph)."""
+        N.check(self._h, self._lib.ptir_set_collect_timings(self._h, int(bool(on))), "set_collect_timings")
+
     def stage_times(self) -> dict:
         """{stage: (milliseconds, launches)} recorded since the previous call (collect_timings=True):
         CUDA events around every launch, on the launch stream."""
