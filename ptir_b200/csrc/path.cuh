@@ -438,50 +438,64 @@ PTIR_DEV bool composite_open(const TraceParams& P, const Composite& c) {
 PTIR_DEV float composite_tmin(const Composite& c) { return c.last_hit + 1e-9f; }
 PTIR_DEV float composite_tend(const Composite& c) { return c.clip_end + 1e-9f; }
 
-// Composite one k-buffer batch. Accepted Gaussians are flagged in `vis` (when given) as int32 1
-// inside the float32 tensor, as the reference does (pathTracer.cuh:283-284).
+// Composite candidate (t, id) of a batch. Accepted Gaussians are flagged in `vis` (when given)
+// as int32 1 inside the float32 tensor, as the reference does (pathTracer.cuh:283-284).
+template <bool kSelfOcc>
+PTIR_DEV void composite_one(const TraceParams& P, TraceCounters& ctr, Composite& c, float t, unsigned id, float* vis) {
+    if (id == kNoHit || !(c.transmittance > P.min_transmittance)) return;
+    if (kSelfOcc && self_occluded(P, t, id, c.d)) {
+        c.last_hit = fmaxf(c.last_hit, t);
+        return;
+    }
+    float dns;
+    const Response r = respond(P, id, c.o, c.d, dns);
+    const bool accept = r.gres > P.min_response && r.alpha > P.alpha_min;
+    if (accept) {
+        ++ctr.accepted;
+        const float w = r.alpha * c.transmittance;
+        const float3 grds = r.scl * r.grd * dot(r.grd, -r.gro);
+        const float hit_t = sqrtf(dot(grds, grds));
+        c.radiance += sh_radiance(P, id, c.d) * w;
+        float3 alb;
+        float rgh, met;
+        load_material(P.part, id, alb, rgh, met);
+        c.albedo += alb * w;
+        c.rough += rgh * w;
+        c.metal += met * w;
+        c.transmittance *= (1.0f - r.alpha);
+        c.depth += hit_t * w;
+        c.hit2 += hit_t * hit_t * w;
+        if (P.flags & kNormals) {
+            c.snrm += load_snrm(P.part, id) * w;
+            const float3 srot = mul_cols(r.rt, r.scl);
+            c.normal += normalize_or_keep((r.gro + r.grd * (dot(r.grd, -r.gro) - sqrtf(9.0f - r.d2))) * srot) * w;
+        }
+        c.hit = true;
+        const float op = 1.0f - c.transmittance;
+        c.distortion = fmaxf(op * c.hit2 - c.depth * c.depth, 0.0f);
+        if (vis) vis[id] = __int_as_float(1);
+    }
+    c.last_hit = fmaxf(c.last_hit, t);
+    if (P.flags & kHitCounts) c.hits_count += accept ? 1.0f : 0.0f;
+}
+
+// Composite one k-buffer batch held in registers.
 template <bool kSelfOcc, int K>
 PTIR_DEV void composite_hits(const TraceParams& P, TraceCounters& ctr, Composite& c, const float (&kt)[K],
                              const unsigned (&kid)[K], float* vis) {
-    const bool normals = (P.flags & kNormals) != 0;
 #pragma unroll
+    for (int i = 0; i < K; ++i) composite_one<kSelfOcc>(P, ctr, c, kt[i], kid[i], vis);
+}
+
+// Composite one k-buffer batch held in memory (entry i at kt[i * stride], kid[i * stride]).
+template <bool kSelfOcc, int K>
+PTIR_DEV void composite_hits_strided(const TraceParams& P, TraceCounters& ctr, Composite& c, const float* kt,
+                                     const unsigned* kid, int stride, float* vis) {
+#pragma unroll 1
     for (int i = 0; i < K; ++i) {
-        const unsigned id = kid[i];
-        if (id == kNoHit || !(c.transmittance > P.min_transmittance)) continue;
-        if (kSelfOcc && self_occluded(P, kt[i], id, c.d)) {
-            c.last_hit = fmaxf(c.last_hit, kt[i]);
-            continue;
-        }
-        float dns;
-        const Response r = respond(P, id, c.o, c.d, dns);
-        const bool accept = r.gres > P.min_response && r.alpha > P.alpha_min;
-        if (accept) {
-            ++ctr.accepted;
-            const float w = r.alpha * c.transmittance;
-            const float3 grds = r.scl * r.grd * dot(r.grd, -r.gro);
-            const float hit_t = sqrtf(dot(grds, grds));
-            c.radiance += sh_radiance(P, id, c.d) * w;
-            float3 alb;
-            float rgh, met;
-            load_material(P.part, id, alb, rgh, met);
-            c.albedo += alb * w;
-            c.rough += rgh * w;
-            c.metal += met * w;
-            c.transmittance *= (1.0f - r.alpha);
-            c.depth += hit_t * w;
-            c.hit2 += hit_t * hit_t * w;
-            if (normals) {
-                c.snrm += load_snrm(P.part, id) * w;
-                const float3 srot = mul_cols(r.rt, r.scl);
-                c.normal += normalize_or_keep((r.gro + r.grd * (dot(r.grd, -r.gro) - sqrtf(9.0f - r.d2))) * srot) * w;
-            }
-            c.hit = true;
-            const float op = 1.0f - c.transmittance;
-            c.distortion = fmaxf(op * c.hit2 - c.depth * c.depth, 0.0f);
-            if (vis) vis[id] = __int_as_float(1);
-        }
-        c.last_hit = fmaxf(c.last_hit, kt[i]);
-        if (P.flags & kHitCounts) c.hits_count += accept ? 1.0f : 0.0f;
+        const unsigned id = kid[i * stride];
+        if (id == kNoHit) break;  // the batch is sorted: the rest is empty too
+        composite_one<kSelfOcc>(P, ctr, c, kt[i * stride], id, vis);
     }
 }
 

@@ -152,17 +152,57 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_sort_keys(TraceParams P, WfV
 
 PTIR_DEV unsigned lanes_below() { return (1u << lane()) - 1u; }
 
+// The compositing accumulators of a lane's segment, parked in shared memory while its warp
+// traverses (they are only touched between trace calls), so that they hold no registers during
+// the traversal: one float per field and thread, field-major (no bank conflicts).
+constexpr int kParkedFields = 22;
+
+struct Parked {
+    float* base;  // this thread's first field
+    int stride;   // threads per block
+    __device__ __forceinline__ float& f(int k) const { return base[k * stride]; }
+    __device__ __forceinline__ void save(const Composite& c) const {
+        f(0) = c.radiance.x; f(1) = c.radiance.y; f(2) = c.radiance.z;
+        f(3) = c.normal.x; f(4) = c.normal.y; f(5) = c.normal.z;
+        f(6) = c.albedo.x; f(7) = c.albedo.y; f(8) = c.albedo.z;
+        f(9) = c.snrm.x; f(10) = c.snrm.y; f(11) = c.snrm.z;
+        f(12) = c.transmittance; f(13) = c.depth; f(14) = c.hit2; f(15) = c.distortion;
+        f(16) = c.hits_count; f(17) = c.rough; f(18) = c.metal; f(19) = c.last_hit; f(20) = c.clip_end;
+        f(21) = c.hit ? 1.0f : 0.0f;
+    }
+    __device__ __forceinline__ void load(Composite& c, float3 o, float3 d) const {
+        c.o = o;
+        c.d = d;
+        c.radiance = make_float3(f(0), f(1), f(2));
+        c.normal = make_float3(f(3), f(4), f(5));
+        c.albedo = make_float3(f(6), f(7), f(8));
+        c.snrm = make_float3(f(9), f(10), f(11));
+        c.transmittance = f(12); c.depth = f(13); c.hit2 = f(14); c.distortion = f(15);
+        c.hits_count = f(16); c.rough = f(17); c.metal = f(18); c.last_hit = f(19); c.clip_end = f(20);
+        c.hit = f(21) != 0.0f;
+    }
+};
+
 // Intersection stage: each lane carries one segment of queue `in_q` (read from `items`, the
 // queue in queue or sorted order) through as many trace calls as it needs (composite_begin /
 // trace / composite_hits / composite_end). A lane whose call has finished composites its batch
 // and starts the next call, or writes its segment, hands it to queue `out_q` (when >= 0) and
 // takes the next one from the queue, so that no lane waits for the slowest segment of its warp.
 // The warp leaves its traversal loop once `refill` lanes wait (a finished call, or idle while
-// the queue still holds segments).
+// the queue still holds segments). Launched with parked_bytes(block, K) of shared memory: the
+// parked accumulators and, while a batch is composited, its k-buffer.
+// Registers per thread of k_wf_trace: 96 lets five 128-thread blocks share an SM (four at the
+// compiler's own choice of 128), which measured 5 % faster on the 1M-Gaussian scene despite a few
+// spills; the 32-entry k-buffer variant keeps more.
+constexpr int trace_regs(int K) { return K > 16 ? 168 : 96; }
+
 template <int K, bool kMark, bool kSelfOcc>
-__global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
-                                                          const unsigned* items, int out_q, unsigned cursor,
-                                                          int refill) {
+__global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
+                                                      const unsigned* items, int out_q, unsigned cursor, int refill) {
+    extern __shared__ float wf_parked[];
+    const Parked pk{wf_parked + threadIdx.x, (int)blockDim.x};
+    float* const batch_t = wf_parked + kParkedFields * blockDim.x + threadIdx.x;
+    unsigned* const batch_id = reinterpret_cast<unsigned*>(batch_t + K * blockDim.x);
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -173,12 +213,12 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* 
     unsigned q = 0;
     int rounds = 0;
     bool drained = false;
-    Composite c;
+    float3 ro = f3(0.0f), rd = f3(0.0f);  // the lane's segment ray
     TraceState t;
     float kt[K];
     unsigned kid[K];
     // next trace call of this lane's segment, or ready with nothing found when it is complete
-    auto next_call = [&]() {
+    auto next_call = [&](const Composite& c) {
         if (!composite_open(P, c)) {
             kid[0] = kNoHit;
             phase = kReady;
@@ -190,8 +230,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* 
             phase = kReady;
             return;
         }
-        phase = trace_start(P.accel, c.o, c.d, composite_tmin(c), composite_tend(c), kt, kid, t, ctr) ? kTracing
-                                                                                                          : kReady;
+        phase = trace_start(P.accel, ro, rd, composite_tmin(c), composite_tend(c), kt, kid, t, ctr) ? kTracing
+                                                                                                      : kReady;
     };
     while (true) {
         // refill the idle lanes
@@ -206,10 +246,14 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* 
                 const unsigned i = base + __popc(idle & lanes_below());
                 if (i < count) {
                     q = items[i];
+                    Composite c;
                     composite_begin(P, c, W.seg[q].o, W.seg[q].d);
+                    ro = c.o;
+                    rd = c.d;
                     ++ctr.segments;
                     rounds = 0;
-                    next_call();
+                    next_call(c);
+                    pk.save(c);
                 }
             }
         }
@@ -223,16 +267,24 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* 
         while (true) {
             const unsigned tracing = __ballot_sync(kFull, phase == kTracing);
             if (!tracing || __popc(eligible & ~tracing) >= refill) break;
-            if (phase == kTracing &&
-                !trace_step(P.accel, c.o, c.d, t, kt, kid, stack, stack_t, P.error_word, ctr))
+            if (phase == kTracing && !trace_step(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr))
                 phase = kReady;
         }
         // composite the finished calls; hand on the finished segments
         bool done = false;
         if (phase == kReady) {
+            Composite c;
+            pk.load(c, ro, rd);
             if (kid[0] != kNoHit) {
-                composite_hits<kSelfOcc>(P, ctr, c, kt, kid, kMark ? vis : nullptr);
-                next_call();
+                // the batch goes to shared memory so that compositing holds no k-buffer registers
+#pragma unroll
+                for (int i = 0; i < K; ++i) {
+                    batch_t[i * blockDim.x] = kt[i];
+                    batch_id[i * blockDim.x] = kid[i];
+                }
+                composite_hits_strided<kSelfOcc, K>(P, ctr, c, batch_t, batch_id, (int)blockDim.x,
+                                                    kMark ? vis : nullptr);
+                next_call(c);
             }
             // nothing found, segment closed, or loop bound: the segment is complete
             if (phase == kReady && kid[0] == kNoHit) {
@@ -243,6 +295,8 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_trace(TraceParams P, float* 
                 store_rng(W, q, rng);
                 phase = kIdle;
                 done = true;
+            } else {
+                pk.save(c);
             }
         }
         if (out_q >= 0) push(W.q[out_q], W.count + out_q, q, done);
@@ -498,7 +552,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_wb_replay(TraceParams P, BwdInp
 }
 
 // persistent grid: resident blocks per SM x SMs
-int grid_for(const void* fn, int block) {
+int grid_for(const void* fn, int block, size_t smem) {
     static int sms = 0;
     if (sms == 0) {
         int dev = 0;
@@ -507,19 +561,22 @@ int grid_for(const void* fn, int block) {
         if (sms <= 0) sms = 148;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, 0) != cudaSuccess || per_sm <= 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, block, smem) != cudaSuccess || per_sm <= 0)
         per_sm = 1;
     return sms * per_sm;
 }
 
+// dynamic shared memory of k_wf_trace<K> at a block size
+size_t parked_bytes(int block, int K) { return sizeof(float) * (kParkedFields + 2 * K) * (size_t)block; }
+
 // grid of a kernel at a block size, computed once per (kernel, block size)
-int grid_cached(const void* fn, int block) {
+int grid_cached(const void* fn, int block, size_t smem = 0) {
     static std::mutex mu;
     static std::map<std::pair<const void*, int>, int> cache;
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find({fn, block});
     if (it != cache.end()) return it->second;
-    const int g = grid_for(fn, block);
+    const int g = grid_for(fn, block, smem);
     cache[{fn, block}] = g;
     return g;
 }
@@ -619,8 +676,8 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
     const int g_primary = grid_cached((const void*)k_wf_fwd_primary<K>, B);
     const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
     const int g_bounce = grid_cached((const void*)k_wf_fwd_bounce<K>, B);
-    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B);
-    const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B);
+    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B, parked_bytes(B, K));
+    const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B, parked_bytes(B, K));
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 2u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
@@ -633,7 +690,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            k_wf_trace<K, true, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, o.visibility, W, kQIsect,
+            k_wf_trace<K, true, false><<<std::min(g_trace0, cap), B, parked_bytes(B, K), s>>>(q, o.visibility, W, kQIsect,
                                                                              W.q[kQIsect], -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
@@ -652,7 +709,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                k_wf_trace<K, true, true><<<g_trace, B, 0, s>>>(q, o.visibility, W, kQIsect, items, kQBounce, cursor,
+                k_wf_trace<K, true, true><<<g_trace, B, parked_bytes(B, K), s>>>(q, o.visibility, W, kQIsect, items, kQBounce, cursor,
                                                                 R);
             });
             ++cursor;
@@ -676,8 +733,8 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
     const int g_primary = grid_cached((const void*)k_wb_primary<K>, B);
     const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
     const int g_bounce = grid_cached((const void*)k_wb_bounce<K>, B);
-    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B);
-    const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B);
+    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B, parked_bytes(B, K));
+    const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B, parked_bytes(B, K));
     const int g_replay = grid_cached((const void*)k_wb_replay<K>, B);
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
@@ -691,7 +748,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            k_wf_trace<K, false, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, nullptr, W, kQIsect, W.q[kQIsect],
+            k_wf_trace<K, false, false><<<std::min(g_trace0, cap), B, parked_bytes(B, K), s>>>(q, nullptr, W, kQIsect, W.q[kQIsect],
                                                                               -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
@@ -715,7 +772,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                k_wf_trace<K, false, true><<<g_trace, B, 0, s>>>(q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
+                k_wf_trace<K, false, true><<<g_trace, B, parked_bytes(B, K), s>>>(q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
             });
             ++cursor;
         }
