@@ -243,6 +243,18 @@ int ptir_debug_accel(ptir_tracer* tracer, float* nodes_host, float* leaves_host,
 int ptir_selective_adam(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, const uint8_t* visible,
                         int64_t n_rows, int32_t row, float lr, float beta1, float beta2, float eps, void* stream);
 
+/* Environment importance table (the tracer's environment_alias input) built on the device:
+ * build_environment_alias_table (threedgrut/model/aliastable.py:244-297) with its Vose alias
+ * construction (aliastable.py:49-116), which the reference runs on the host every few training
+ * steps. environment: [env_h, env_w, channels >= 3] float32; an equirect map is area-averaged to
+ * table_h x table_w (the reference's 64 x 128), a cube map (env_h == 6 env_w) is used at its
+ * own size. table_out: [3, h, w] float32 = probability, alias index (as float), pdf per
+ * steradian. scratch: device memory of ptir_env_table_scratch_bytes(h * w) bytes, reused per
+ * call. Asynchronous on `stream`; needs no tracer. */
+size_t ptir_env_table_scratch_bytes(int32_t cells);
+int ptir_build_env_table(const float* environment, int32_t env_h, int32_t env_w, int32_t channels, int32_t table_h,
+                         int32_t table_w, float* table_out, void* scratch, size_t scratch_bytes, void* stream);
+
 const char* ptir_last_error(const ptir_tracer* tracer);
 
 /* Allocation-free scene bounds. This entry point has no counterpart in the reference.

@@ -109,7 +109,8 @@ class PtirCounters(C.Structure):
 
 EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", "ptir_trace", "ptir_trace_bwd",
            "ptir_trace_views", "ptir_trace_bwd_views", "ptir_get_counters", "ptir_get_stage_counters", "ptir_get_stage_times", "ptir_set_collect_timings", "ptir_device_status",
-           "ptir_scene_bounds", "ptir_debug_accel", "ptir_selective_adam", "ptir_last_error")
+           "ptir_scene_bounds", "ptir_debug_accel", "ptir_selective_adam", "ptir_env_table_scratch_bytes",
+           "ptir_build_env_table", "ptir_last_error")
 
 
 def lib_path() -> str:
@@ -162,6 +163,11 @@ def load(build_if_missing: bool = True):
     L.ptir_selective_adam.argtypes = [_FP, _FP, _FP, _FP, _FP, C.c_int64, C.c_int32, C.c_float, C.c_float, C.c_float,
                                       C.c_float, C.c_void_p]
     L.ptir_selective_adam.restype = C.c_int
+    L.ptir_env_table_scratch_bytes.argtypes = [C.c_int32]
+    L.ptir_env_table_scratch_bytes.restype = C.c_size_t
+    L.ptir_build_env_table.argtypes = [_FP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _FP, _FP,
+                                       C.c_size_t, C.c_void_p]
+    L.ptir_build_env_table.restype = C.c_int
     L.ptir_last_error.argtypes = [C.c_void_p]
     L.ptir_last_error.restype = C.c_char_p
     _LIB = L

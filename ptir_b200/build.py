@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_PATH = os.path.join(HERE, "libptir_b200.so")
-SOURCES = ("api.cu", "accel.cu", "tracer.cu", "wavefront.cu", "stages.cu", "storage.cu", "optim.cu")
+SOURCES = ("api.cu", "accel.cu", "tracer.cu", "wavefront.cu", "stages.cu", "storage.cu", "optim.cu", "envtable.cu")
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-lineinfo", "--use_fast_math", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

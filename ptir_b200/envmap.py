@@ -88,6 +88,27 @@ def build(environment: torch.Tensor, cube: bool | None = None, size=ALIAS_TABLE_
                 pdf=pdf.reshape(-1).contiguous())
 
 
+def build_device(environment: torch.Tensor, size=ALIAS_TABLE_SIZE) -> torch.Tensor:
+    """The packed [3, h, w] table of build() + pack(), computed on the environment's CUDA device
+    by the library (ptir_build_env_table): same algorithm and Vose order, float64 on the device."""
+    from . import _native as N
+
+    env = environment.detach()
+    if env.dtype != torch.float32 or not env.is_cuda or env.dim() != 3 or env.shape[2] < 3:
+        raise ValueError("build_device: a [H, W, C>=3] float32 CUDA tensor is required")
+    env = env.contiguous()
+    H, W, Ch = (int(v) for v in env.shape)
+    h, w = (H, W) if H == 6 * W else (int(size[0]), int(size[1]))
+    lib = N.load()
+    scratch = torch.empty(int(lib.ptir_env_table_scratch_bytes(h * w)), dtype=torch.uint8, device=env.device)
+    out = torch.empty((3, h, w), dtype=torch.float32, device=env.device)
+    rc = lib.ptir_build_env_table(env.data_ptr(), H, W, Ch, h, w, out.data_ptr(), scratch.data_ptr(),
+                                  scratch.numel(), torch.cuda.current_stream(env.device).cuda_stream)
+    if rc != N.PTIR_OK:
+        raise N.PtirError(rc, "ptir_build_env_table failed")
+    return out
+
+
 def pack(table: dict, device=None) -> torch.Tensor:
     """[3, h, w] float32: prob, alias index as float, pdf."""
     h, w = table["height"], table["width"]
