@@ -246,6 +246,42 @@ def algorithmic_bytes(fc: dict, bc: dict, samples: int):
     return fwd, bwd
 
 
+def tune_launch_shape(S, args, device) -> dict:
+    """Autotune k-buffer, block, chunk and refill on a sample of the workload (a sixteenth of its
+    rays, forward + adjoint), cached in _autotune.json beside this file."""
+    from ptir_b200 import autotune
+
+    tr0 = S.tracer(storage=args.storage)
+    tr0.build_bvh(S.pos, S.rot, S.scl, S.dns, True, True)
+    del tr0
+    if S.batched:
+        frame, t2w, z, h, w = S.views[0]
+        n = z * h * w
+        ori, drs = S.ray_ori[:n], S.ray_dir[:n]
+        views = [S.views[0]]
+    else:
+        z = max(1, S.ray_ori.shape[0] // 16)
+        ori, drs, views = S.ray_ori[:z], S.ray_dir[:z], None
+
+    def run(tr):
+        tr.build_bvh(S.pos, S.rot, S.scl, S.dns, True, True)
+        scene = (S.density, S.material, S.sph, S.snrm, S.env, S.alias, *S.lights, 0, 3, 0.001, S.wl.max_bounces)
+        f = tr.trace_views(views, ori, drs, *scene) if views else tr.trace(0, S.t2w, ori, drs, *scene)
+        z_ = torch.zeros_like
+        g = torch.sign(f[10] - 0.5) * 1e-6
+        args_b = (*f[:8], f[10], f[11], *scene[:12], z_(f[0]), z_(f[1]), z_(f[2]), z_(f[3]), z_(f[4]), z_(f[5]),
+                  z_(f[6]), z_(f[7]), g, z_(f[11]), *scene[12:])
+        if views:
+            tr.trace_bwd_views(views, ori, drs, *args_b)
+        else:
+            tr.trace_bwd(0, S.t2w, ori, drs, *args_b)
+
+    sig = f"{S.wl.name}|n={S.wl.n}|samples={S.samples}|bounces={S.wl.max_bounces}|storage={args.storage}"
+    tuner = autotune.Autotuner(os.path.join(ROOT, "_autotune.json"))
+    best, _ = tuner.tune(sig, lambda **kw: S.tracer(storage=args.storage, **kw), run)
+    return best.launch()
+
+
 def _view_config(views):
     if all(v == views[0] for v in views):
         return {"resolution": list(views[0][:2]), "spp": views[0][2]}
@@ -256,7 +292,10 @@ def run_ours(args, rank, world, device):
     import torch.distributed as dist
 
     S = Setup(workload_of(args), rank, device)
-    tr = S.tracer(collect_timings=True, storage=args.storage)
+    shape = {}
+    if args.autotune:
+        shape = tune_launch_shape(S, args, device)
+    tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     # target image: the same scene with albedo perturbed by N(0, 0.02)
     gen = torch.Generator(device="cpu").manual_seed(1234)
@@ -440,6 +479,7 @@ def run_ours(args, rank, world, device):
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": S.wl.name, "storage": args.storage, "gaussians": S.wl.n,
+                   "launch": shape or "defaults",
                    "views_per_gpu": len(S.wl.views), **_view_config(S.wl.views),
                    "max_bounces": S.wl.max_bounces, "env": list(S.wl.env_hw), "cuda_graph": bool(args.graph),
                    "samples_per_gpu": S.samples, "segments_per_step_per_gpu": segs,
@@ -519,6 +559,8 @@ def main():
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--graph", action="store_true", help="capture the training iteration in a CUDA graph")
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick k-buffer, block, chunk and refill by a timed sweep on a sample of the workload")
     ap.add_argument("--storage", default="bf16", choices=("fp32", "bf16", "fp16"),
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
