@@ -576,6 +576,8 @@ int grid_cached(const void* fn, int block, size_t smem = 0) {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find({fn, block});
     if (it != cache.end()) return it->second;
+    // more than the default 48 KB of dynamic shared memory needs the kernel's opt-in
+    if (smem > 48 * 1024) cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int g = grid_for(fn, block, smem);
     cache[{fn, block}] = g;
     return g;

@@ -133,3 +133,18 @@ def test_wavefront_and_megakernel_agree(cuda_device, chunk_tiles, kbuffer):
     for a, b in zip(grads["megakernel"], grads["wavefront"]):
         a, b = a.double().reshape(-1), b.double().reshape(-1)
         assert (a - b).norm() <= tol * b.norm() + 1e-12
+
+
+@pytest.mark.parametrize("block_size,kbuffer,refill", [(256, 16, 32), (64, 16, 8), (256, 32, 16), (256, 8, 32)])
+def test_launch_shapes(cuda_device, block_size, kbuffer, refill):
+    """Block size and refill threshold change no forward output; every k-buffer size launches at
+    every block size (the 256-thread blocks need more than 48 KB of shared memory)."""
+    s = small_scene(n=2500, w=40, h=36, spp=2, max_bounces=4)
+    S = to_torch(s)
+    ref = [t.clone() for t in gpu_trace(make_tracer(kbuffer=kbuffer), S)]
+    tr = make_tracer(kbuffer=kbuffer, block_size=block_size, refill_lanes=refill)
+    out = gpu_trace(tr, S)
+    torch.cuda.synchronize()
+    assert tr.device_status() == 0
+    for k, (a, b) in enumerate(zip(ref, out)):
+        assert torch.equal(a, b), k
