@@ -38,12 +38,12 @@ PTIR_DEV void kbuf_clear(float (&kt)[K], unsigned (&kid)[K]) {
     }
 }
 
-// number of filled slots
+// number of filled slots (a filled slot has a distance below kFarT)
 template <int K>
-PTIR_DEV unsigned kbuf_count(const unsigned (&kid)[K]) {
+PTIR_DEV unsigned kbuf_count(const float (&kt)[K]) {
     unsigned c = 0;
 #pragma unroll
-    for (int j = 0; j < K; ++j) c += kid[j] != kNoHit ? 1u : 0u;
+    for (int j = 0; j < K; ++j) c += kt[j] < kFarT ? 1u : 0u;
     return c;
 }
 
@@ -84,9 +84,9 @@ PTIR_DEV float min3f(float a, float b, float c) {
 }
 
 // exact instance test of leaf record p
-template <int K>
+template <int K, class Ids>
 PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
-                        unsigned (&kid)[K]) {
+                        Ids& kid) {
     const float4* rec = A.leaves + 4 * (size_t)p;
     const float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
     const float3 od = make_float3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w,
@@ -119,16 +119,16 @@ struct TraceState {
 
 // Start a trace call of ray (o, d) over (tmin, tend). Returns true when node visits remain
 // (trace_step), false when (kt, kid) is already final.
-template <int K>
-PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
-                          unsigned (&kid)[K], TraceState& t, TraceCounters& ctr) {
+template <int K, class Ids>
+PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K], Ids& kid,
+                          TraceState& t, TraceCounters& ctr) {
     kbuf_clear(kt, kid);
     ++ctr.calls;
     if (A.n <= 0) return false;
     if (A.n == 1) {
         ++ctr.leaves;
         test_leaf(A, 0, o, d, tmin, tend, kt, kid);
-        ctr.candidates += kbuf_count(kid);
+        ctr.candidates += kbuf_count(kt);
         return false;
     }
     t.inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -140,9 +140,9 @@ PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, fl
 }
 
 // One 4-wide node visit of a trace call. Returns false when the call is complete.
-template <int K>
-PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], unsigned (&kid)[K],
-                         int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
+template <int K, class Ids>
+PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid, int* stack,
+                         float* stack_t, unsigned* err, TraceCounters& ctr) {
     const float3 inv = t.inv;
     const float tmin = t.tmin, tend = t.tend;
     int sp = t.sp;
@@ -205,7 +205,7 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
             const int np = __popc(inner);
             if (sp + np > kStackDepth) {
                 atomicOr(err, kErrStackOverflow);
-                ctr.candidates += kbuf_count(kid);
+                ctr.candidates += kbuf_count(kt);
                 return false;
             }
             while (inner) {
@@ -237,7 +237,7 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
                 }
             }
             if (!found) {
-                ctr.candidates += kbuf_count(kid);
+                ctr.candidates += kbuf_count(kt);
                 return false;
             }
         }

@@ -193,7 +193,8 @@ struct Parked {
 // parked accumulators and, while a batch is composited, its k-buffer.
 // Registers per thread of k_wf_trace: 96 lets five 128-thread blocks share an SM (four at the
 // compiler's own choice of 128), which measured 5 % faster on the 1M-Gaussian scene despite a few
-// spills; the 32-entry k-buffer variant keeps more.
+// spills; the 32-entry k-buffer variant gets 168 (three blocks: keeping its ids in shared memory
+// instead, for four blocks, measured slower).
 constexpr int trace_regs(int K) { return K > 16 ? 168 : 96; }
 
 template <int K, bool kMark, bool kSelfOcc>
@@ -215,18 +216,18 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
     bool drained = false;
     float3 ro = f3(0.0f), rd = f3(0.0f);  // the lane's segment ray
     TraceState t;
-    float kt[K];
+    float kt[K];  // a call found nothing when kt[0] == kFarT
     unsigned kid[K];
     // next trace call of this lane's segment, or ready with nothing found when it is complete
     auto next_call = [&](const Composite& c) {
         if (!composite_open(P, c)) {
-            kid[0] = kNoHit;
+            kt[0] = kFarT;
             phase = kReady;
             return;
         }
         if (++rounds > kMaxRounds + 1) {
             atomicOr(P.error_word, kErrLoopBound);
-            kid[0] = kNoHit;
+            kt[0] = kFarT;
             phase = kReady;
             return;
         }
@@ -275,8 +276,8 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
         if (phase == kReady) {
             Composite c;
             pk.load(c, ro, rd);
-            if (kid[0] != kNoHit) {
-                // the batch goes to shared memory so that compositing holds no k-buffer registers
+            if (kt[0] < kFarT) {
+                // the batch goes to shared memory, so compositing holds no k-buffer registers
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
                     batch_t[i * blockDim.x] = kt[i];
@@ -287,7 +288,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
                 next_call(c);
             }
             // nothing found, segment closed, or loop bound: the segment is complete
-            if (phase == kReady && kid[0] == kNoHit) {
+            if (phase == kReady && kt[0] >= kFarT) {
                 Segment s;
                 Pcg32 rng = load_rng(W, q);
                 composite_end(P, c, W.seg[q].scatter_pdf, W.seg[q].light_pdf, s, rng);
