@@ -247,8 +247,10 @@ def algorithmic_bytes(fc: dict, bc: dict, samples: int):
 
 
 def tune_launch_shape(S, args, device) -> dict:
-    """Autotune k-buffer, block, chunk and refill on a sample of the workload (a sixteenth of its
-    rays, forward + adjoint), cached in _autotune.json beside this file."""
+    """Autotune the launch shape on a sample of the workload (a thirty-second of its rays, or its
+    first view; forward + adjoint), cached in _autotune.json beside this file. --autotune-full
+    sweeps k-buffer, block, chunk and refill; the default sweep is k-buffer {16, 32} x block
+    {64, 128}."""
     from ptir_b200 import autotune
 
     tr0 = S.tracer(storage=args.storage)
@@ -260,7 +262,7 @@ def tune_launch_shape(S, args, device) -> dict:
         ori, drs = S.ray_ori[:n], S.ray_dir[:n]
         views = [S.views[0]]
     else:
-        z = max(1, S.ray_ori.shape[0] // 16)
+        z = max(1, S.ray_ori.shape[0] // 32)
         ori, drs, views = S.ray_ori[:z], S.ray_dir[:z], None
 
     def run(tr):
@@ -276,9 +278,12 @@ def tune_launch_shape(S, args, device) -> dict:
         else:
             tr.trace_bwd(0, S.t2w, ori, drs, *args_b)
 
-    sig = f"{S.wl.name}|n={S.wl.n}|samples={S.samples}|bounces={S.wl.max_bounces}|storage={args.storage}"
+    shapes = autotune.space() if args.autotune_full else autotune.space(kbuffers=(16, 32), blocks=(64, 128),
+                                                                          chunks=(131072,), refills=(32,))
+    sig = (f"{S.wl.name}|n={S.wl.n}|samples={S.samples}|bounces={S.wl.max_bounces}|storage={args.storage}"
+           f"|shapes={len(shapes)}")
     tuner = autotune.Autotuner(os.path.join(ROOT, "_autotune.json"))
-    best, _ = tuner.tune(sig, lambda **kw: S.tracer(storage=args.storage, **kw), run)
+    best, _ = tuner.tune(sig, lambda **kw: S.tracer(storage=args.storage, **kw), run, shapes=shapes)
     return best.launch()
 
 
@@ -293,7 +298,7 @@ def run_ours(args, rank, world, device):
 
     S = Setup(workload_of(args), rank, device)
     shape = {}
-    if args.autotune:
+    if not args.no_autotune:
         shape = tune_launch_shape(S, args, device)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
@@ -559,8 +564,9 @@ def main():
     ap.add_argument("--spp", type=int, default=None)
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
     ap.add_argument("--graph", action="store_true", help="capture the training iteration in a CUDA graph")
-    ap.add_argument("--autotune", action="store_true",
-                    help="pick k-buffer, block, chunk and refill by a timed sweep on a sample of the workload")
+    ap.add_argument("--no-autotune", action="store_true", help="use the default launch shape (k-buffer 16)")
+    ap.add_argument("--autotune-full", action="store_true",
+                    help="sweep k-buffer, block, chunk and refill (default: k-buffer and block)")
     ap.add_argument("--storage", default="bf16", choices=("fp32", "bf16", "fp16"),
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
