@@ -11,6 +11,10 @@
 #include "storage.cuh"
 #include "wavefront.h"
 
+namespace ptir {
+cudaError_t launch_fold(float* out, const float* comp, long long n, cudaStream_t s);  // optim.cu
+}
+
 static_assert(PTIR_MAX_VIEWS == ptir::kMaxViews, "view table size of the C ABI");
 static_assert(sizeof(ptir::TraceParams) <= 4000, "kernel parameters must stay within 4 KB");
 static_assert((int)PTIR_STAGE_INTERSECT == (int)ptir::kStageIntersect &&
@@ -29,6 +33,8 @@ struct ptir_tracer {
     uint4* hot = nullptr;     // 16-bit attribute records (storage != FP32)
     uint4* cold = nullptr;
     size_t attr_capacity = 0;  // Gaussians the record buffers hold
+    float* comp = nullptr;     // compensation terms of the gradient sums
+    size_t comp_capacity = 0;  // floats
     unsigned* error_word = nullptr;
     unsigned long long* counters = nullptr;  // [kNumStages][kNumCounters]
     std::string last_error;
@@ -252,6 +258,7 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     if (!(config->block_size == 0 || config->block_size == 64 || config->block_size == 128 || config->block_size == 256))
         return PTIR_EINVAL;
     if (config->ray_order != 0 && config->ray_order != 1) return PTIR_EINVAL;
+    if (config->grad_sums != 0 && config->grad_sums != 1) return PTIR_EINVAL;
     if (config->storage != PTIR_STORAGE_FP32 && config->storage != PTIR_STORAGE_BF16 &&
         config->storage != PTIR_STORAGE_FP16)
         return PTIR_EINVAL;
@@ -280,6 +287,7 @@ void ptir_destroy(ptir_tracer* t) {
     cudaFree(t->counters);
     cudaFree(t->hot);
     cudaFree(t->cold);
+    cudaFree(t->comp);
     delete t;
 }
 
@@ -373,7 +381,7 @@ int trace_bwd_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* vi
         e = cudaMemsetAsync(t->counters, 0, kCounterBytes, s);
         if (e != cudaSuccess) return cuda_fail(t, e, "clear counters");
     }
-    ptir::BwdInputs bi;
+    ptir::BwdInputs bi{};
     bi.pbr = b->pbr;
     bi.light = b->light;
     bi.pbr_grad = b->pbr_grad;
@@ -381,11 +389,34 @@ int trace_bwd_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* vi
     bi.material_grad = b->material_grad;
     bi.particle_material_grad = o->particle_material_grad;
     bi.environment_grad = env ? o->environment_grad : nullptr;
+    // compensation buffers of the Kahan-pair gradient sums: [n,5] then [eh,ew,4], zeroed per call
+    const size_t n_mat = a->n > 0 ? 5 * (size_t)a->n : 0;
+    const size_t n_env = bi.environment_grad ? 4 * (size_t)p.env.w * p.env.h : 0;
+    const bool comp = t->cfg.grad_sums == 0 && n_mat + n_env > 0;
+    if (comp) {
+        if (n_mat + n_env > t->comp_capacity) {
+            if (t->comp) e = cudaFreeAsync(t->comp, s);
+            t->comp = nullptr;
+            t->comp_capacity = 0;
+            e = cudaMallocAsync(reinterpret_cast<void**>(&t->comp), sizeof(float) * (n_mat + n_env), s);
+            if (e != cudaSuccess) return cuda_fail(t, e, "allocate gradient compensation");
+            t->comp_capacity = n_mat + n_env;
+        }
+        e = cudaMemsetAsync(t->comp, 0, sizeof(float) * (n_mat + n_env), s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "clear gradient compensation");
+        bi.particle_material_comp = n_mat ? t->comp : nullptr;
+        bi.environment_comp = n_env ? t->comp + n_mat : nullptr;
+    }
     const ptir::StageCtx sc = stage_ctx(t);
     e = t->cfg.schedule == PTIR_SCHEDULE_MEGAKERNEL
             ? ptir::launch_trace_bwd(p, bi, sc, s)
             : ptir::launch_trace_bwd_wavefront(p, bi, t->wave, tuning_of(t->cfg), sc, s);
     if (e != cudaSuccess) return cuda_fail(t, e, "trace_bwd launch");
+    if (comp) {
+        if (n_mat) e = ptir::launch_fold(bi.particle_material_grad, bi.particle_material_comp, (long long)n_mat, s);
+        if (e == cudaSuccess && n_env) e = ptir::launch_fold(bi.environment_grad, bi.environment_comp, (long long)n_env, s);
+        if (e != cudaSuccess) return cuda_fail(t, e, "fold gradient compensation");
+    }
     return PTIR_OK;
 }
 

@@ -116,6 +116,8 @@ struct BwdInputs {
     const float* material_grad;  // [z,h,w,5]
     float* particle_material_grad;  // [n,5]
     float* environment_grad;        // [eh,ew,4]
+    float* particle_material_comp;  // [n,5] compensation terms of the material gradient sums, or null
+    float* environment_comp;        // [eh,ew,4] compensation terms of the environment sums, or null
 };
 
 enum Counter : int {

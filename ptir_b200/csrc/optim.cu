@@ -28,7 +28,20 @@ __global__ void k_selective_adam(float* __restrict__ param, const float* __restr
     }
 }
 
+__global__ void k_fold(float* __restrict__ out, const float* __restrict__ comp, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] += comp[i];
+}
+
 }  // namespace
+
+// out[i] += comp[i]: the compensation terms of Kahan-pair gradient sums folded into the sums
+cudaError_t launch_fold(float* out, const float* comp, long long n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    const long long blocks = (n + 255) / 256;
+    k_fold<<<(unsigned)(blocks < 148LL * 32 ? blocks : 148LL * 32), 256, 0, s>>>(out, comp, n);
+    return cudaGetLastError();
+}
 
 }  // namespace ptir
 

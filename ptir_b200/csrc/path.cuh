@@ -551,6 +551,20 @@ PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
 }
 
 // ------------------------------------------------------------------------------------
+// Gradient scatter: a float atomic add, and with a compensation buffer the rounding error of
+// that add (TwoSum of the value found and the term, in round-to-nearest) added to the buffer,
+// so that sum + compensation carries the terms to about twice float precision however many
+// paths hit the same Gaussian or texel.
+PTIR_DEV void grad_add(float* g, float* comp, float v) {
+    const float old = atomicAdd(g, v);
+    if (!comp) return;
+    const float s = __fadd_rn(old, v);
+    const float bp = __fsub_rn(s, old);
+    const float err = __fadd_rn(__fsub_rn(old, __fsub_rn(s, bp)), __fsub_rn(v, bp));
+    if (err != 0.0f) atomicAdd(comp, err);
+}
+
+// ------------------------------------------------------------------------------------
 // backward: path replay ("radiative backprop") of referenceBwdOptix.cu:27-74
 
 // One re-traversal of a segment that scatters a material gradient onto its Gaussians
@@ -603,11 +617,12 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const Repla
                 ++C.ctr.replay_accepted;
                 const float w = r.alpha * tr;
                 float* g = B.particle_material_grad + 5 * (size_t)id;
-                atomicAdd(g + 0, w * da.x);
-                atomicAdd(g + 1, w * da.y);
-                atomicAdd(g + 2, w * da.z);
-                atomicAdd(g + 3, w * dr);
-                if (metallic_on) atomicAdd(g + 4, w * dm);
+                float* cg = B.particle_material_comp ? B.particle_material_comp + 5 * (size_t)id : nullptr;
+                grad_add(g + 0, cg ? cg + 0 : nullptr, w * da.x);
+                grad_add(g + 1, cg ? cg + 1 : nullptr, w * da.y);
+                grad_add(g + 2, cg ? cg + 2 : nullptr, w * da.z);
+                grad_add(g + 3, cg ? cg + 3 : nullptr, w * dr);
+                if (metallic_on) grad_add(g + 4, cg ? cg + 4 : nullptr, w * dm);
                 tr *= (1.0f - r.alpha);
             }
             start = fmaxf(start, kt[i]);
@@ -626,10 +641,12 @@ PTIR_DEV float3 env_radiance_bwd(const Ctx& C, const BwdInputs& B, float3 d, flo
     ++C.ctr.env;
     if (B.environment_grad) {
         auto add = [&](int x, int y, float w) {
-            float* g = B.environment_grad + 4 * ((size_t)y * E.w + x);
-            atomicAdd(g + 0, w * cg.x);
-            atomicAdd(g + 1, w * cg.y);
-            atomicAdd(g + 2, w * cg.z);
+            const size_t texel = 4 * ((size_t)y * E.w + x);
+            float* g = B.environment_grad + texel;
+            float* c = B.environment_comp ? B.environment_comp + texel : nullptr;
+            grad_add(g + 0, c ? c + 0 : nullptr, w * cg.x);
+            grad_add(g + 1, c ? c + 1 : nullptr, w * cg.y);
+            grad_add(g + 2, c ? c + 2 : nullptr, w * cg.z);
         };
         add(f.x0, f.y0, f.w00);
         add(f.x1, f.y0, f.w10);

@@ -53,7 +53,9 @@ class OptixTracer:
     traversal), ``refill_lanes`` (waiting lanes before an intersection warp refills, 1..32) and
     ``block_size`` (64, 128 or 256); 0 keeps the default. ``collect_timings`` records CUDA events
     around every kernel launch for ``stage_times()``; ``sort_rays`` intersects bounce rays in
-    (direction octant, origin cell) order (the results do not change). ``storage`` ("fp32",
+    (direction octant, origin cell) order (the results do not change); ``compensated_grads``
+    accumulates the gradient atomics as Kahan pairs (off: plain float atomics, as the
+    reference). ``storage`` ("fp32",
     "bf16" or "fp16") sets how the tracer holds the Gaussians' attributes: in 16-bit storage
     geometry, material, shading normals and SH are rounded once per call (and by ``build_bvh``)
     and widened on load, all arithmetic staying FP32."""
@@ -82,6 +84,7 @@ class OptixTracer:
         block_size: int = 0,
         collect_timings: bool = False,
         sort_rays: bool = True,
+        compensated_grads: bool = True,
         storage: str = "fp32",
     ):
         if pipeline not in ("reference",):
@@ -98,7 +101,7 @@ class OptixTracer:
             self.sph_degree, int(bool(enable_normals)), int(bool(enable_hit_counts)), int(bool(enable_mis)),
             int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
             N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
-            int(bool(collect_timings)), 0 if sort_rays else 1, N.STORAGES[storage])
+            int(bool(collect_timings)), 0 if sort_rays else 1, 0 if compensated_grads else 1, N.STORAGES[storage])
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:
