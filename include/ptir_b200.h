@@ -72,6 +72,11 @@ typedef struct ptir_config {
     int32_t collect_timings;      /* record CUDA events around every kernel launch (ptir_get_stage_times) */
     int32_t ray_order;            /* wavefront bounce rays: 0 = intersected in (direction octant, origin cell)
                                      order (default), 1 = in queue order; results are the same */
+    int32_t exact_replay;         /* 0 = backward re-traversals end where the reference's do (its float epsilon
+                                     leaves out each segment's last composited Gaussian), 1 = they include
+                                     it, which makes the adjoint the exact derivative of the same-sample
+                                     estimator for albedo and the environment (no counterpart in the
+                                     reference) */
     int32_t grad_sums;            /* gradient scatter: 0 = compensated (Kahan-pair) float atomics (default),
                                      1 = plain float atomics as the reference */
     int32_t storage;              /* attribute storage: PTIR_STORAGE_FP32 (the caller's tensors are read as

@@ -39,6 +39,7 @@ class PtirConfig(C.Structure):
         ("block_size", C.c_int32),
         ("collect_timings", C.c_int32),
         ("ray_order", C.c_int32),
+        ("exact_replay", C.c_int32),
         ("grad_sums", C.c_int32),
         ("storage", C.c_int32),
     ]

@@ -79,6 +79,7 @@ unsigned flags_of(const ptir_config& c) {
     if (c.enable_mis) f |= ptir::kMis;
     if (c.enable_metallic) f |= ptir::kMetallic;
     if (c.visualize_lights) f |= ptir::kVisualizeLights;
+    if (c.exact_replay) f |= ptir::kExactReplay;
     return f;
 }
 

@@ -42,6 +42,7 @@ enum Flags : unsigned {
     kMis = 4u,
     kMetallic = 8u,
     kVisualizeLights = 16u,
+    kExactReplay = 32u,  // backward re-traversals include the segment's last composited Gaussian
 };
 
 struct ParticleView {

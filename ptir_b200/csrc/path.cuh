@@ -592,7 +592,11 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const Repla
     const bool metallic_on = (P.flags & kMetallic) != 0;
     const float2 clip = clip_scene(P, o, d);
     float start = fmaxf(0.0f, clip.x - 1e-9f);
-    const float end = fminf(max_hit, clip.y) + 1e-9f;
+    // The reference ends the re-traversal at max_hit + 1e-9 in float: beyond t ~ 0.017 that is
+    // max_hit itself, and with the strict t < tend test the segment's last composited Gaussian
+    // gets no gradient. kExactReplay extends the end by one float step to include it.
+    const float end = (P.flags & kExactReplay) ? nextafterf(fminf(max_hit, clip.y), 3.0e38f)
+                                               : fminf(max_hit, clip.y) + 1e-9f;
     float tr = 1.0f;
     float kt[Ctx::K];
     unsigned kid[Ctx::K];

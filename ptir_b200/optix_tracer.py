@@ -53,7 +53,9 @@ class OptixTracer:
     traversal), ``refill_lanes`` (waiting lanes before an intersection warp refills, 1..32) and
     ``block_size`` (64, 128 or 256); 0 keeps the default. ``collect_timings`` records CUDA events
     around every kernel launch for ``stage_times()``; ``sort_rays`` intersects bounce rays in
-    (direction octant, origin cell) order (the results do not change); ``compensated_grads``
+    (direction octant, origin cell) order (the results do not change); ``exact_replay`` lets the
+    backward re-traversals include each segment's last composited Gaussian, which the
+    reference's float epsilon leaves out; ``compensated_grads``
     accumulates the gradient atomics as Kahan pairs (off: plain float atomics, as the
     reference). ``storage`` ("fp32",
     "bf16" or "fp16") sets how the tracer holds the Gaussians' attributes: in 16-bit storage
@@ -84,6 +86,7 @@ class OptixTracer:
         block_size: int = 0,
         collect_timings: bool = False,
         sort_rays: bool = True,
+        exact_replay: bool = False,
         compensated_grads: bool = True,
         storage: str = "fp32",
     ):
@@ -101,7 +104,8 @@ class OptixTracer:
             self.sph_degree, int(bool(enable_normals)), int(bool(enable_hit_counts)), int(bool(enable_mis)),
             int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
             N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
-            int(bool(collect_timings)), 0 if sort_rays else 1, 0 if compensated_grads else 1, N.STORAGES[storage])
+            int(bool(collect_timings)), 0 if sort_rays else 1, int(bool(exact_replay)), 0 if compensated_grads else 1,
+            N.STORAGES[storage])
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:
