@@ -83,10 +83,10 @@ PTIR_DEV float min3f(float a, float b, float c) {
     return r;
 }
 
-// exact instance test of leaf record p
-template <int K, class Ids>
-PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
-                        Ids& kid) {
+// Exact instance test of leaf record p against ray (o, d) over (tmin, min(tend, cut)): true with
+// the candidate's distance and Gaussian id when it is one.
+PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float cut,
+                             float& ts_out, unsigned& id_out) {
     const float4* rec = A.leaves + 4 * (size_t)p;
     const float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
     const float3 od = make_float3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w,
@@ -97,16 +97,26 @@ PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmi
     const float dd2 = dot(dd, dd);
     const float den = 1.0f / dd2;
     const float ts = -dot(od, dd) * den;
-    if (!(ts > tmin && ts < tend && ts < kt[K - 1])) return;
+    if (!(ts > tmin && ts < tend && ts < cut)) return false;
     // object-space unit box within [tmin, tend]
     const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float b0, b1;
     slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
-    if (fmaxf(b0, tmin) > fminf(b1, tend)) return;
+    if (fmaxf(b0, tmin) > fminf(b1, tend)) return false;
     const float3 c = cross(normalize_or_keep(dd), od);
-    if (!(dot(c, c) * den < 9.0f)) return;
-    const unsigned gid = __float_as_uint(__ldg(&rec[3].x));
-    kbuf_insert(kt, kid, ts, gid);
+    if (!(dot(c, c) * den < 9.0f)) return false;
+    ts_out = ts;
+    id_out = __float_as_uint(__ldg(&rec[3].x));
+    return true;
+}
+
+// exact instance test of leaf record p, inserted into the k-buffer when it is a candidate
+template <int K, class Ids>
+PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
+                        Ids& kid) {
+    float ts;
+    unsigned gid;
+    if (leaf_candidate(A, p, o, d, tmin, tend, kt[K - 1], ts, gid)) kbuf_insert(kt, kid, ts, gid);
 }
 
 // A trace call in progress: the next node to visit and the stack depth (the stack itself is
@@ -139,112 +149,135 @@ PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, fl
     return true;
 }
 
-// One 4-wide node visit of a trace call. Returns false when the call is complete.
-template <int K, class Ids>
-PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid, int* stack,
-                         float* stack_t, unsigned* err, TraceCounters& ctr) {
+// One 4-wide node visit between its box tests and its descent, so that the leaf children can be
+// tested in between (in the lane, or by the whole warp).
+struct NodeVisit {
+    int ch[4];           // children: >= 0 node, kNoChild empty, else leaf ~c
+    float t0[4], key[4]; // clipped entry distance, middle of the clipped interval (x2)
+    unsigned hits;       // children whose box the ray crosses in front of the K-th distance
+};
+
+// Box tests of the node t.node. Returns the mask of leaf children to test.
+template <int K>
+PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, const TraceState& t, const float (&kt)[K], NodeVisit& v,
+                             TraceCounters& ctr) {
     const float3 inv = t.inv;
     const float tmin = t.tmin, tend = t.tend;
+    ++ctr.nodes;
+    const float4* nd = A.nodes + 8 * (size_t)t.node;
+    // near and far plane rows of each axis from the direction's signs (rows: lo.x lo.y lo.z
+    // hi.x hi.y hi.z), so each slab interval needs no min / max of its two plane distances
+    const int rx = inv.x >= 0.0f ? 0 : 3, ry = inv.y >= 0.0f ? 1 : 4, rz = inv.z >= 0.0f ? 2 : 5;
+    const float4 nx = __ldg(nd + rx), ny = __ldg(nd + ry), nz = __ldg(nd + rz);
+    const float4 fx = __ldg(nd + (3 - rx)), fy = __ldg(nd + (5 - ry)), fz = __ldg(nd + (7 - rz));
+    const float4 cc = __ldg(nd + 6);
+    const float nxa[4] = {nx.x, nx.y, nx.z, nx.w}, nya[4] = {ny.x, ny.y, ny.z, ny.w};
+    const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fxa[4] = {fx.x, fx.y, fx.z, fx.w};
+    const float fya[4] = {fy.x, fy.y, fy.z, fy.w}, fza[4] = {fz.x, fz.y, fz.z, fz.w};
+    v.ch[0] = __float_as_int(cc.x);
+    v.ch[1] = __float_as_int(cc.y);
+    v.ch[2] = __float_as_int(cc.z);
+    v.ch[3] = __float_as_int(cc.w);
+    v.hits = 0;
+    unsigned leaves = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        // clipped slab interval [a, b]; a NaN plane distance (0 * inf) leaves its axis unbounded
+        const float a = max3f((nxa[k] - o.x) * inv.x, (nya[k] - o.y) * inv.y, fmaxf((nza[k] - o.z) * inv.z, tmin));
+        const float b = min3f((fxa[k] - o.x) * inv.x, (fya[k] - o.y) * inv.y, fminf((fza[k] - o.z) * inv.z, tend));
+        v.t0[k] = a;
+        // nearer middle of the clipped interval first: boxes that contain the origin all
+        // enter at tmin, their extent along the ray tells them apart
+        v.key[k] = a + b;
+        const bool h = v.ch[k] != kNoChild && a <= b && a <= kt[K - 1];
+        v.hits |= h ? (1u << k) : 0u;
+        leaves |= (h && v.ch[k] < 0) ? (1u << k) : 0u;
+    }
+    return leaves;
+}
+
+// Descent after the leaf tests: into the nearest internal child still in front of the K-th
+// distance, the others pushed farthest first; else the next stacked subtree that can still hold
+// a nearer candidate. Returns false when the call is complete.
+template <int K>
+PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], int* stack, float* stack_t,
+                      unsigned* err, TraceCounters& ctr) {
     int sp = t.sp;
     int node = t.node;
-    {
-        ++ctr.nodes;
-        const float4* nd = A.nodes + 8 * (size_t)node;
-        // near and far plane rows of each axis from the direction's signs (rows: lo.x lo.y lo.z
-        // hi.x hi.y hi.z), so each slab interval needs no min / max of its two plane distances
-        const int rx = inv.x >= 0.0f ? 0 : 3, ry = inv.y >= 0.0f ? 1 : 4, rz = inv.z >= 0.0f ? 2 : 5;
-        const float4 nx = __ldg(nd + rx), ny = __ldg(nd + ry), nz = __ldg(nd + rz);
-        const float4 fx = __ldg(nd + (3 - rx)), fy = __ldg(nd + (5 - ry)), fz = __ldg(nd + (7 - rz));
-        const float4 cc = __ldg(nd + 6);
-        const float nxa[4] = {nx.x, nx.y, nx.z, nx.w}, nya[4] = {ny.x, ny.y, ny.z, ny.w};
-        const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fxa[4] = {fx.x, fx.y, fx.z, fx.w};
-        const float fya[4] = {fy.x, fy.y, fy.z, fy.w}, fza[4] = {fz.x, fz.y, fz.z, fz.w};
-        const int ch[4] = {__float_as_int(cc.x), __float_as_int(cc.y), __float_as_int(cc.z), __float_as_int(cc.w)};
-        float t0[4], key[4];
-        bool hit[4];
+    int best = -1;
+    float bkey = 3.0e38f;
+    unsigned inner = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            // clipped slab interval [a, b]; a NaN plane distance (0 * inf) leaves its axis unbounded
-            const float a =
-                max3f((nxa[k] - o.x) * inv.x, (nya[k] - o.y) * inv.y, fmaxf((nza[k] - o.z) * inv.z, tmin));
-            const float b =
-                min3f((fxa[k] - o.x) * inv.x, (fya[k] - o.y) * inv.y, fminf((fza[k] - o.z) * inv.z, tend));
-            t0[k] = a;
-            // nearer middle of the clipped interval first: boxes that contain the origin all
-            // enter at tmin, their extent along the ray tells them apart
-            key[k] = a + b;
-            hit[k] = ch[k] != kNoChild && a <= b && a <= kt[K - 1];
+    for (int k = 0; k < 4; ++k) {
+        const bool h = ((v.hits >> k) & 1u) && v.ch[k] >= 0 && v.t0[k] <= kt[K - 1];
+        inner |= h ? (1u << k) : 0u;
+        if (h && v.key[k] < bkey) {
+            bkey = v.key[k];
+            best = k;
         }
-        // leaf children: one test call site, looping over the hit mask
-        unsigned leaves = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) leaves |= (hit[k] && ch[k] < 0) ? (1u << k) : 0u;
-        while (leaves) {
-            const int k = __ffs(leaves) - 1;
-            leaves &= leaves - 1;
-            const int c = k == 0 ? ch[0] : (k == 1 ? ch[1] : (k == 2 ? ch[2] : ch[3]));
-            ++ctr.leaves;
-            test_leaf(A, ~c, o, d, tmin, tend, kt, kid);
+    }
+    if (best >= 0) {
+        inner &= ~(1u << best);
+        const int np = __popc(inner);
+        if (sp + np > kStackDepth) {
+            atomicOr(err, kErrStackOverflow);
+            ctr.candidates += kbuf_count(kt);
+            return false;
         }
-        // the internal children still in front of the K-th distance: descend into the nearest,
-        // push the others farthest first so that the nearest of them is popped first
-        int best = -1;
-        float bkey = 3.0e38f;
-        unsigned inner = 0;
+        while (inner) {
+            // farthest remaining first
+            int far = -1;
+            float fkey = -3.0e38f;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const bool h = hit[k] && ch[k] >= 0 && t0[k] <= kt[K - 1];
-            inner |= h ? (1u << k) : 0u;
-            if (h && key[k] < bkey) {
-                bkey = key[k];
-                best = k;
-            }
-        }
-        if (best >= 0) {
-            inner &= ~(1u << best);
-            const int np = __popc(inner);
-            if (sp + np > kStackDepth) {
-                atomicOr(err, kErrStackOverflow);
-                ctr.candidates += kbuf_count(kt);
-                return false;
-            }
-            while (inner) {
-                // farthest remaining first
-                int far = -1;
-                float fkey = -3.0e38f;
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if ((inner >> k) & 1u && key[k] > fkey) {
-                        fkey = key[k];
-                        far = k;
-                    }
-                }
-                inner &= ~(1u << far);
-                stack[sp] = far == 0 ? ch[0] : (far == 1 ? ch[1] : (far == 2 ? ch[2] : ch[3]));
-                stack_t[sp] = far == 0 ? t0[0] : (far == 1 ? t0[1] : (far == 2 ? t0[2] : t0[3]));
-                ++sp;
-            }
-            node = best == 0 ? ch[0] : (best == 1 ? ch[1] : (best == 2 ? ch[2] : ch[3]));
-        } else {
-            // pop the next subtree that can still hold a candidate nearer than the K-th
-            bool found = false;
-            while (sp > 0) {
-                --sp;
-                if (stack_t[sp] <= kt[K - 1]) {
-                    node = stack[sp];
-                    found = true;
-                    break;
+            for (int k = 0; k < 4; ++k) {
+                if ((inner >> k) & 1u && v.key[k] > fkey) {
+                    fkey = v.key[k];
+                    far = k;
                 }
             }
-            if (!found) {
-                ctr.candidates += kbuf_count(kt);
-                return false;
+            inner &= ~(1u << far);
+            stack[sp] = far == 0 ? v.ch[0] : (far == 1 ? v.ch[1] : (far == 2 ? v.ch[2] : v.ch[3]));
+            stack_t[sp] = far == 0 ? v.t0[0] : (far == 1 ? v.t0[1] : (far == 2 ? v.t0[2] : v.t0[3]));
+            ++sp;
+        }
+        node = best == 0 ? v.ch[0] : (best == 1 ? v.ch[1] : (best == 2 ? v.ch[2] : v.ch[3]));
+    } else {
+        // pop the next subtree that can still hold a candidate nearer than the K-th
+        bool found = false;
+        while (sp > 0) {
+            --sp;
+            if (stack_t[sp] <= kt[K - 1]) {
+                node = stack[sp];
+                found = true;
+                break;
             }
+        }
+        if (!found) {
+            ctr.candidates += kbuf_count(kt);
+            return false;
         }
     }
     t.sp = sp;
     t.node = node;
     return true;
+}
+
+// One 4-wide node visit of a trace call with its leaf tests in the lane. Returns false when the
+// call is complete.
+template <int K, class Ids>
+PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid, int* stack,
+                         float* stack_t, unsigned* err, TraceCounters& ctr) {
+    NodeVisit v;
+    unsigned leaves = visit_node(A, o, t, kt, v, ctr);
+    // leaf children: one test call site, looping over the mask
+    while (leaves) {
+        const int k = __ffs(leaves) - 1;
+        leaves &= leaves - 1;
+        const int c = k == 0 ? v.ch[0] : (k == 1 ? v.ch[1] : (k == 2 ? v.ch[2] : v.ch[3]));
+        ++ctr.leaves;
+        test_leaf(A, ~c, o, d, t.tmin, t.tend, kt, kid);
+    }
+    return descend(t, v, kt, stack, stack_t, err, ctr);
 }
 
 // Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
