@@ -101,3 +101,30 @@ def test_compensated_gradient_sums(cuda_device):
     a, b = res[True]
     spread = np.abs(a - b) / np.maximum(np.abs(a), 1e-30)
     assert float(np.quantile(spread, 0.999)) <= 2.5e-7, float(np.quantile(spread, 0.999))
+
+
+def test_backward_sh_indirect_mode(cuda_device):
+    """The adjoint in RenderOpts.INDIRECT mode (environment.cuh:733-760) against the oracle."""
+    s = small_scene(n=2000, w=40, h=32, spp=2, max_bounces=3, sh_full=True)
+    s["render_opts"] = 1
+    cfg = O.OracleConfig()
+    ref, _, _ = O.trace(cfg, s, "f64")
+    rng = np.random.default_rng(13)
+    zhw = s["ray_ori"].shape[:3]
+    grads = dict(pbr=rng.standard_normal(zhw + (3,)).astype(np.float32),
+                 light=0.1 * rng.standard_normal(zhw + (3,)).astype(np.float32),
+                 material=rng.standard_normal(zhw + (5,)).astype(np.float32))
+    mg_ref, eg_ref, _ = O.trace_bwd(cfg, s, ref, grads, "f64")
+    tr = make_tracer()
+    S = to_torch(s)
+    fwd = list(gpu_trace(tr, S))
+    fwd[10] = torch.from_numpy(ref["pbr"]).cuda()
+    fwd[11] = torch.from_numpy(ref["light"]).cuda()
+    g = {k: torch.from_numpy(v).cuda() for k, v in grads.items()}
+    _, mg, _, _, eg = gpu_trace_bwd(tr, S, fwd, g["pbr"], g["light"], g["material"])
+    torch.cuda.synchronize()
+    assert tr.device_status() == 0
+    rel, cos = _rel_cos(mg.cpu().numpy()[:, :4], mg_ref[:, :4])
+    assert rel <= 2e-3 and cos >= 0.999, ("material", rel, cos)
+    rel, cos = _rel_cos(eg.cpu().numpy()[..., :3], eg_ref[..., :3])
+    assert rel <= 2e-3 and cos >= 0.999, ("environment", rel, cos)

@@ -148,3 +148,23 @@ def test_launch_shapes(cuda_device, block_size, kbuffer, refill):
     assert tr.device_status() == 0
     for k, (a, b) in enumerate(zip(ref, out)):
         assert torch.equal(a, b), k
+
+
+@pytest.mark.parametrize("schedule", ["wavefront", "megakernel"])
+def test_sh_indirect_mode(cuda_device, schedule):
+    """RenderOpts.INDIRECT (sh_indirect = 1): secondary hits take the Gaussians' SH radiance as
+    indirect light and paths stop after two bounces (environment.cuh:650-683,
+    optixTracer.cpp:959). Forward outputs against the oracle with the usual tolerances."""
+    s = small_scene(n=2000, w=40, h=32, spp=2, max_bounces=4, sh_full=True)
+    s["render_opts"] = 1
+    ref, _, _ = O.trace(O.OracleConfig(), s, "f64")
+    tr = make_tracer(schedule=schedule)
+    out = _gpu_outputs(gpu_trace(tr, to_torch(s)))
+    torch.cuda.synchronize()
+    assert tr.device_status() == 0
+    for k in ("radiance", "density", "material"):
+        assert _close_frac(out[k], ref[k]) >= 0.995, k
+    for k in ("pbr", "light", "components"):
+        assert _close_frac(out[k], ref[k]) >= 0.99, k
+        m_ref, m_gpu = float(ref[k].mean()), float(out[k].mean())
+        assert abs(m_gpu - m_ref) <= 1e-2 * max(abs(m_ref), 1e-3) + 1e-4, (k, m_gpu, m_ref)
