@@ -35,7 +35,7 @@
 extern "C" {
 #endif
 
-#define PTIR_ABI_VERSION 2
+#define PTIR_ABI_VERSION 3
 
 enum {
     PTIR_OK = 0,
@@ -72,11 +72,13 @@ typedef struct ptir_config {
     int32_t collect_timings;      /* record CUDA events around every kernel launch (ptir_get_stage_times) */
     int32_t ray_order;            /* wavefront bounce rays: 0 = intersected in (direction octant, origin cell)
                                      order (default), 1 = in queue order; results are the same */
-    int32_t exact_replay;         /* 0 = backward re-traversals end where the reference's do (its float epsilon
-                                     leaves out each segment's last composited Gaussian), 1 = they include
-                                     it, which makes the adjoint the exact derivative of the same-sample
-                                     estimator for albedo and the environment (no counterpart in the
-                                     reference) */
+    int32_t exact_replay;         /* 0 = the reference's adjoint: backward re-traversals end where its float
+                                     epsilon leaves out each segment's last composited Gaussian, and the
+                                     NEE albedo term is weighted by the environment's radiance whatever
+                                     light was sampled; 1 = re-traversals include that Gaussian and the
+                                     NEE term uses the sampled light's radiance, which makes the adjoint
+                                     the exact derivative of the same-sample estimator for albedo and
+                                     the environment (no counterpart in the reference) */
     int32_t grad_sums;            /* gradient scatter: 0 = compensated (Kahan-pair) float atomics (default),
                                      1 = plain float atomics as the reference */
     int32_t storage;              /* attribute storage: PTIR_STORAGE_FP32 (the caller's tensors are read as
@@ -106,8 +108,22 @@ typedef struct ptir_trace_args {
     int32_t env_h, env_w;
     const float* environment_alias; /* [3,AH,AW] prob/alias/pdf or NULL */
     int32_t alias_h, alias_w;
-    /* punctual / area light tables (tracer.py:40-119 LightBuffers); counts must be 0 */
+    /* Punctual and area lights: the LightBuffers tensors (tracer.py:40-119), float32 / int32,
+     * row-major, as the reference's light sampler reads them (lightSampler.cuh, meshLight.cuh).
+     * With num_light_entries == 0 the environment is the only light, as in the reference. */
+    const float* lights;              /* [num_lights, 9]: type (1 point, 2 sphere), position xyz, radius,
+                                         radiance rgb, two_sided */
+    const float* light_alias;         /* [5, num_light_entries]: alias prob, alias entry, light type
+                                         (0 environment, 1 point, 2 sphere, 3 mesh), light index,
+                                         selection pdf */
+    const float* mesh_light_vertices; /* [num_mesh_light_vertices, 3] */
+    const int32_t* mesh_light_triangles; /* [num_mesh_light_triangles, 3] vertex indices */
+    const float* mesh_lights;         /* [num_mesh_lights, 8]: triangle offset, triangle count, vertex
+                                         offset, vertex count, radiance rgb, two_sided */
+    const float* mesh_light_alias;    /* [3, mesh_light_alias_cols]: alias prob, alias (local to the
+                                         mesh), area pdf per triangle */
     int32_t num_lights, num_light_entries, num_mesh_lights;
+    int32_t num_mesh_light_vertices, num_mesh_light_triangles, mesh_light_alias_cols;
     uint32_t sh_indirect;           /* RenderOpts: 0 = NONE, 1 = INDIRECT */
     int32_t sph_eval_degree;        /* SH degree evaluated (<= sph_degree) */
     float min_transmittance;        /* render.min_transmittance */

@@ -831,30 +831,323 @@ public:
         }
         return env.pdf[size_t(y) * env.aw + x];
     }
-    // lightSampler.cuh:385-406 (no top-level table: environment only)
-    T light_pdf(V3<T> wi) const { return env.has_light() ? alias_pdf(wi) : T(0); }
+    // ---- punctual and area lights (lightSampler.cuh:12-406, meshLight.cuh:11-101)
+    struct LightSample {
+        V3<T> wi{}, Li{};
+        T pdf = 0, dist = T(1e20);
+        unsigned type = 0;  // 0 environment, 1 point, 2 sphere, 3 mesh
+    };
+    // the reference's static_cast<unsigned>(v + 0.5f) on the device: toward zero, saturating, NaN -> 0
+    static unsigned table_index(float v) {
+        const float f = v + 0.5f;
+        if (!(f > 0.0f)) return 0u;
+        if (f >= 4294967296.0f) return 0xFFFFFFFFu;
+        return unsigned(f);
+    }
+    static unsigned scaled_index(float u, unsigned n) {  // min(unsigned(u * n), n - 1)
+        const float f = u * float(n);
+        const unsigned i = !(f > 0.0f) ? 0u : (f >= 4294967296.0f ? 0xFFFFFFFFu : unsigned(f));
+        return std::min(i, n - 1u);
+    }
+    bool has_table() const { return in.light_entries > 0; }
+    bool has_mesh() const {
+        return in.num_mesh_lights > 0 && in.num_mesh_vertices > 0 && in.num_mesh_triangles > 0 &&
+               in.mesh_tri_cols >= in.num_mesh_triangles;
+    }
+    float table(int row, unsigned e) const { return in.light_table[size_t(row) * in.light_entries + e]; }
+    float tri_table(int row, unsigned t) const { return in.mesh_tri_table[size_t(row) * in.mesh_tri_cols + t]; }
+    const float* light_row(unsigned id) const { return in.lights + 9 * size_t(id); }
+    const float* mesh_row(unsigned id) const { return in.mesh_lights + 8 * size_t(id); }
+    unsigned light_type(unsigned id) const {
+        return id < unsigned(in.num_lights) ? table_index(light_row(id)[0]) : 0xFFFFFFFFu;
+    }
+    static V3<T> f3(const float* p) { return {T(p[0]), T(p[1]), T(p[2])}; }
+    static T length(V3<T> v) { return std::sqrt(dot(v, v)); }
+
+    // lightSampler.cuh:59-72
+    unsigned sample_entry(Sampler& s) const {
+        const unsigned n = unsigned(in.light_entries);
+        const unsigned first = scaled_index(s.next_1d(), n);
+        const unsigned other = std::min(table_index(table(1, first)), n - 1u);
+        return s.next_1d() < table(0, first) ? first : other;
+    }
+    // lightSampler.cuh:74-91
+    LightSample sample_env_light(Sampler& s, T select) {
+        LightSample ls;
+        if (!env.has_light()) return ls;
+        T epdf = 0;
+        ls.wi = sample_alias_dir(s, epdf);
+        ls.Li = background(ls.wi);
+        ls.pdf = select * epdf;
+        return ls;
+    }
+    // lightSampler.cuh:93-123
+    LightSample sample_point(V3<T> pos, unsigned id, T select) const {
+        LightSample ls;
+        if (id >= unsigned(in.num_lights) || light_type(id) != 1u || select <= T(0)) return ls;
+        const float* r = light_row(id);
+        const V3<T> to = f3(r + 1) - pos;
+        const T d2 = dot(to, to);
+        if (d2 <= T(1e-12)) return ls;
+        const T dist = std::sqrt(d2);
+        ls.wi = to / dist;
+        ls.Li = f3(r + 5) / d2;
+        ls.pdf = select;
+        ls.dist = dist;
+        ls.type = 1;
+        return ls;
+    }
+    // lightSampler.cuh:125-179
+    LightSample sample_sphere(V3<T> pos, Sampler& s, unsigned id, T select) const {
+        LightSample ls;
+        if (id >= unsigned(in.num_lights) || light_type(id) != 2u) return ls;
+        const float* r = light_row(id);
+        const T radius = T(r[4]);
+        if (radius <= T(0)) return ls;
+        const float u1 = s.next_1d();
+        const float u2 = s.next_1d();
+        const T z = T(1) - T(2) * T(u1);
+        const T rr = std::sqrt(std::fmax(T(0), T(1) - z * z));
+        const T phi = T(2) * T(kPi) * T(u2);
+        const V3<T> nrm{rr * std::cos(phi), rr * std::sin(phi), z};
+        const V3<T> to = (f3(r + 1) + nrm * radius) - pos;
+        const T d2 = dot(to, to);
+        if (d2 <= T(1e-12)) return ls;
+        const T dist = std::sqrt(d2);
+        const V3<T> wi = to / dist;
+        const T cl = std::fabs(dot(nrm, -wi));
+        if (cl <= T(1e-6)) return ls;
+        const T area = T(4) * T(kPi) * radius * radius;
+        ls.wi = wi;
+        ls.Li = f3(r + 5);
+        ls.pdf = select * (T(1) / std::fmax(area, T(1e-12))) * d2 / cl;
+        ls.dist = dist;
+        ls.type = 2;
+        return ls;
+    }
+    // lightSampler.cuh:181-222
+    T sphere_pdf(V3<T> pos, V3<T> wi, unsigned id) const {
+        if (id >= unsigned(in.num_lights) || light_type(id) != 2u) return T(0);
+        const float* r = light_row(id);
+        const T radius = T(r[4]);
+        if (radius <= T(0)) return T(0);
+        const V3<T> oc = pos - f3(r + 1);
+        const T b = dot(oc, wi);
+        const T c = dot(oc, oc) - radius * radius;
+        const T disc = b * b - c;
+        if (disc <= T(0)) return T(0);
+        T t = -b - std::sqrt(disc);
+        if (t <= T(1e-6)) t = -b + std::sqrt(disc);
+        if (t <= T(1e-6)) return T(0);
+        const V3<T> n = safe_normalize((pos + wi * t) - f3(r + 1));
+        const T cl = std::fabs(dot(n, -wi));
+        if (cl <= T(1e-6)) return T(0);
+        const T area = T(4) * T(kPi) * radius * radius;
+        return (T(1) / std::fmax(area, T(1e-12))) * (t * t) / cl;
+    }
+    // meshLight.cuh:18-51
+    bool mesh_triangle(unsigned tri, V3<T>& v0, V3<T>& v1, V3<T>& v2) const {
+        if (tri >= unsigned(in.num_mesh_triangles)) return false;
+        const int* t = in.mesh_triangles + 3 * size_t(tri);
+        if (t[0] < 0 || t[1] < 0 || t[2] < 0) return false;
+        const unsigned nv = unsigned(in.num_mesh_vertices);
+        if (unsigned(t[0]) >= nv || unsigned(t[1]) >= nv || unsigned(t[2]) >= nv) return false;
+        v0 = f3(in.mesh_vertices + 3 * size_t(t[0]));
+        v1 = f3(in.mesh_vertices + 3 * size_t(t[1]));
+        v2 = f3(in.mesh_vertices + 3 * size_t(t[2]));
+        return true;
+    }
+    // meshLight.cuh:53-84
+    static bool intersect_triangle(V3<T> o, V3<T> d, V3<T> v0, V3<T> v1, V3<T> v2, T& t) {
+        const V3<T> e1 = v1 - v0, e2 = v2 - v0;
+        const V3<T> pv = cross(d, e2);
+        const T det = dot(e1, pv);
+        if (std::fabs(det) <= T(1e-8)) return false;
+        const T inv = T(1) / det;
+        const V3<T> tv = o - v0;
+        const T u = dot(tv, pv) * inv;
+        if (u < T(0) || u > T(1)) return false;
+        const V3<T> qv = cross(tv, e1);
+        const T v = dot(d, qv) * inv;
+        if (v < T(0) || (u + v) > T(1)) return false;
+        t = dot(e2, qv) * inv;
+        return t > T(1e-5);
+    }
+    // triangle range of a mesh light (checked in 64 bits)
+    bool mesh_range(unsigned id, unsigned& off, unsigned& count) const {
+        const float* m = mesh_row(id);
+        off = table_index(m[0]);
+        count = table_index(m[1]);
+        return count != 0u && uint64_t(off) + count <= uint64_t(in.num_mesh_triangles);
+    }
+    // cosine at the light; ok = false for a degenerate triangle
+    static T mesh_cosine(V3<T> v0, V3<T> v1, V3<T> v2, V3<T> wi, bool two_sided, bool& ok) {
+        const V3<T> nu = cross(v1 - v0, v2 - v0);
+        const T nl = length(nu);
+        ok = nl > T(1e-12);
+        if (!ok) return T(0);
+        const T c = dot(nu / nl, -wi);
+        return two_sided ? std::fabs(c) : c;
+    }
+    // meshLight.cuh:86-101
+    unsigned sample_triangle(Sampler& s, unsigned off, unsigned count) const {
+        const unsigned first = off + scaled_index(s.next_1d(), count);
+        const unsigned other = std::min(table_index(tri_table(1, first)), count - 1u);
+        return s.next_1d() < tri_table(0, first) ? first : off + other;
+    }
+    // lightSampler.cuh:224-293
+    LightSample sample_mesh(V3<T> pos, Sampler& s, unsigned id, T select) const {
+        LightSample ls;
+        if (!has_mesh() || id >= unsigned(in.num_mesh_lights) || select <= T(0)) return ls;
+        unsigned off, count;
+        if (!mesh_range(id, off, count)) return ls;
+        const unsigned tri = sample_triangle(s, off, count);
+        V3<T> v0, v1, v2;
+        if (!mesh_triangle(tri, v0, v1, v2)) return ls;
+        float u = s.next_1d();
+        float v = s.next_1d();
+        if (u + v > 1.0f) { u = 1.0f - u; v = 1.0f - v; }
+        const V3<T> to = (v0 + (v1 - v0) * T(u) + (v2 - v0) * T(v)) - pos;
+        const T d2 = dot(to, to);
+        if (d2 <= T(1e-12)) return ls;
+        const T dist = std::sqrt(d2);
+        const V3<T> wi = to / dist;
+        bool ok;
+        const T cl = mesh_cosine(v0, v1, v2, wi, mesh_row(id)[7] > 0.5f, ok);
+        if (!ok || cl <= T(1e-6)) return ls;
+        ls.wi = wi;
+        ls.Li = f3(mesh_row(id) + 4);
+        ls.pdf = select * T(tri_table(2, tri)) * d2 / cl;
+        ls.dist = dist;
+        ls.type = 3;
+        return ls;
+    }
+    // lightSampler.cuh:295-338
+    T mesh_pdf(V3<T> pos, V3<T> wi, unsigned id) const {
+        if (!has_mesh() || id >= unsigned(in.num_mesh_lights)) return T(0);
+        unsigned off, count;
+        if (!mesh_range(id, off, count)) return T(0);
+        const bool two = mesh_row(id)[7] > 0.5f;
+        T pdf = 0;
+        for (unsigned tri = off; tri < off + count; ++tri) {
+            V3<T> v0, v1, v2;
+            T t;
+            if (!mesh_triangle(tri, v0, v1, v2) || !intersect_triangle(pos, wi, v0, v1, v2, t)) continue;
+            bool ok;
+            const T cl = mesh_cosine(v0, v1, v2, wi, two, ok);
+            if (!ok || cl <= T(1e-6)) continue;
+            pdf += T(tri_table(2, tri)) * (t * t) / cl;
+        }
+        return pdf;
+    }
+    // lightSampler.cuh:340-383
+    LightSample sample_light(V3<T> pos, Sampler& s) {
+        if (!has_table()) return sample_env_light(s, T(1));
+        const unsigned e = sample_entry(s);
+        const unsigned type = table_index(table(2, e)), id = table_index(table(3, e));
+        const T select = T(table(4, e));
+        switch (type) {
+        case 0: return sample_env_light(s, select);
+        case 1: return sample_point(pos, id, select);
+        case 2: return sample_sphere(pos, s, id, select);
+        case 3: return sample_mesh(pos, s, id, select);
+        default: return LightSample();
+        }
+    }
+    // lightSampler.cuh:385-406 (point lights are delta lights and add nothing)
+    T light_pdf(V3<T> pos, V3<T> wi) const {
+        if (!has_table()) return env.has_light() ? alias_pdf(wi) : T(0);
+        T pdf = 0;
+        for (unsigned i = 0; i < unsigned(in.light_entries); ++i) {
+            const T select = T(table(4, i));
+            if (select <= T(0)) continue;
+            const unsigned type = table_index(table(2, i)), id = table_index(table(3, i));
+            T p = 0;
+            if (type == 0) p = env.has_light() ? alias_pdf(wi) : T(0);
+            else if (type == 2) p = sphere_pdf(pos, wi, id);
+            else if (type == 3) p = mesh_pdf(pos, wi, id);
+            pdf += select * p;
+        }
+        return pdf;
+    }
+    // environment.cuh:491-536
+    bool hit_sphere_light(const Ray<T>& r, unsigned id, T& t, V3<T>& rad) const {
+        if (light_type(id) != 2u) return false;
+        const float* L = light_row(id);
+        const T radius = T(L[4]);
+        if (radius <= T(0)) return false;
+        const V3<T> oc = r.o - f3(L + 1);
+        const T b = dot(oc, r.d);
+        const T c = dot(oc, oc) - radius * radius;
+        const T disc = b * b - c;
+        if (disc <= T(0)) return false;
+        const T sq = std::sqrt(disc);
+        t = -b - sq;
+        if (t <= T(1e-5)) t = -b + sq;
+        if (t <= T(1e-5)) return false;
+        rad = f3(L + 5);
+        return !(rad.x <= T(0) && rad.y <= T(0) && rad.z <= T(0));
+    }
+    // environment.cuh:538-597
+    bool hit_mesh_light(const Ray<T>& r, unsigned id, T& t, V3<T>& rad) const {
+        if (!has_mesh()) return false;
+        unsigned off, count;
+        if (!mesh_range(id, off, count)) return false;
+        rad = f3(mesh_row(id) + 4);
+        if (rad.x <= T(0) && rad.y <= T(0) && rad.z <= T(0)) return false;
+        const bool two = mesh_row(id)[7] > 0.5f;
+        T nearest = T(1e20);
+        for (unsigned tri = off; tri < off + count; ++tri) {
+            V3<T> v0, v1, v2;
+            T th;
+            if (!mesh_triangle(tri, v0, v1, v2) || !intersect_triangle(r.o, r.d, v0, v1, v2, th)) continue;
+            bool ok;
+            const T cl = mesh_cosine(v0, v1, v2, r.d, two, ok);
+            if (!ok || cl <= T(1e-6)) continue;
+            nearest = std::fmin(nearest, th);
+        }
+        if (nearest >= T(1e19)) return false;
+        t = nearest;
+        return true;
+    }
+    // environment.cuh:599-634: what an escaped ray sees. 0 nothing, 1 a sphere or mesh light
+    // (render.visualize_lights only; radiance in rad), 2 the environment
+    int escaped_light(const Ray<T>& r, V3<T>& rad) const {
+        if (cfg.visualize_lights) {
+            T nearest = T(1e20);
+            bool found = false;
+            for (unsigned i = 0; i < unsigned(in.num_lights); ++i) {
+                T t; V3<T> c;
+                if (hit_sphere_light(r, i, t, c) && t < nearest) { nearest = t; rad = c; found = true; }
+            }
+            for (unsigned i = 0; i < unsigned(in.num_mesh_lights); ++i) {
+                T t; V3<T> c;
+                if (hit_mesh_light(r, i, t, c) && t < nearest) { nearest = t; rad = c; found = true; }
+            }
+            if (found) return 1;
+        }
+        return env.has_env() ? 2 : 0;
+    }
 
     static T mis(T a, T b) { const T a2 = a * a, b2 = b * b; return a2 / std::fmax(a2 + b2, T(1e-6)); }
 
     // pathTracer.cuh:461-504 (+ lightSampler.cuh:74-91, 359-383)
     void sample_nee(Path<T>& P, Sampler& s) {
         const Interaction<T> it = P.cur.inter;
-        T lpdf = 0, spdf = 0;
-        V3<T> wi{}, Li{};
-        if (env.has_light()) {
-            T epdf = 0;
-            wi = sample_alias_dir(s, epdf);
-            Li = background(wi);
-            lpdf = epdf;
-        }
+        T spdf = 0;
+        const LightSample ls = sample_light(it.position, s);
+        const T lpdf = ls.pdf;
+        const V3<T> wi = ls.wi, Li = ls.Li;
         if (lpdf <= T(0) || is_zero(Li)) { P.emitter = RayPayload<T>(); return; }
         if (dot(it.snormal, wi) <= T(0)) { P.emitter = RayPayload<T>(); return; }
         V3<T> n, wo, alb; T met;
         frame_of(it, P.cur.ray.d, n, wo, alb, met);
         const V3<T> bc = eval_brdf(wo, n, alb, met, clamp_rough(it.roughness), wi, spdf);
+        if (ls.type == 1u) spdf = T(0);
         const Ray<T> lr{it.position + wi * T(2e-2), wi};
+        const T tmax = ls.dist < T(1e19) ? std::fmax(T(0), ls.dist - T(2e-2)) : T(1e20);
         st.segments++;
-        if (shadow_occluded(lr, s, T(0), T(1e20))) { P.emitter = RayPayload<T>(); return; }
+        if (shadow_occluded(lr, s, T(0), tmax)) { P.emitter = RayPayload<T>(); return; }
         P.emitter = RayPayload<T>(lr, T(0));
         P.emitter.light_pdf = lpdf;
         P.emitter.scatter_pdf = spdf;
@@ -877,7 +1170,7 @@ public:
         P.throughput = nt;
         const Ray<T> nr{it.position + safe_normalize(next) * T(2e-2), next};
         P.cur = RayPayload<T>(nr, T(0));
-        if (cfg.enable_mis) { P.cur.scatter_pdf = spdf; P.cur.light_pdf = light_pdf(next); }
+        if (cfg.enable_mis) { P.cur.scatter_pdf = spdf; P.cur.light_pdf = light_pdf(it.position, next); }
     }
 
     // environment.cuh:636-715
@@ -898,8 +1191,10 @@ public:
                 P.acc += P.cur.contribution;
                 P.acc_indirect += P.cur.contribution;
             } else if (P.cur.valid) {
-                if (!env.has_env()) return;
-                const V3<T> vr = background(P.cur.ray.d);
+                V3<T> vr{};
+                const int seen = escaped_light(P.cur.ray, vr);
+                if (seen == 0) return;
+                if (seen == 2) vr = background(P.cur.ray.d);
                 P.throughput *= P.cur.transmittance;
                 P.cur.light += vr;
                 P.acc_light += vr;
@@ -912,8 +1207,10 @@ public:
         }
         if (cfg.enable_mis && first) { P.acc += nee; P.acc_direct += nee; }
         if (P.cur.valid) {
-            if (!env.has_env()) return;
-            const V3<T> vr = background(P.cur.ray.d);
+            V3<T> vr{};
+            const int seen = escaped_light(P.cur.ray, vr);
+            if (seen == 0) return;
+            if (seen == 2) vr = background(P.cur.ray.d);
             P.throughput *= P.cur.transmittance;
             P.cur.light += vr;
             P.acc_light += vr;
@@ -1007,7 +1304,7 @@ public:
         T lpdf = 0;
         bool first_nee = false;
         if (cfg.enable_mis) {
-            lpdf = light_pdf(next);
+            lpdf = light_pdf(it.position, next);
             first_nee = P.bounces == 1u && vmax(nt) >= T(1e-4);
             if (first_nee) nee_grad_bwd(P, cr, it);
         }
@@ -1050,12 +1347,14 @@ public:
                 if (cfg.enable_mis && first) P.cur.contribution *= bmis;
                 P.acc -= P.cur.contribution;
             } else if (P.cur.valid) {
-                if (!env.has_env()) return;
+                V3<T> vr{};
+                const int seen = escaped_light(P.cur.ray, vr);
+                if (seen == 0) return;
                 P.throughput *= P.cur.transmittance;
                 V3<T> eg = P.acc_grad * P.throughput;
                 if (cfg.enable_mis && first) eg *= bmis;
                 eg += P.acc_light_grad;
-                const V3<T> vr = background_bwd(P.cur.ray.d, eg, &P.cur.ray_dir_grad);
+                if (seen == 2) vr = background_bwd(P.cur.ray.d, eg, &P.cur.ray_dir_grad);
                 P.cur.contribution = P.throughput * vr;
                 if (cfg.enable_mis && first) P.cur.contribution *= bmis;
                 P.acc -= P.cur.contribution;
@@ -1064,12 +1363,14 @@ public:
         }
         if (cfg.enable_mis && first) P.acc -= P.emitter.contribution * lmis;
         if (P.cur.valid) {
-            if (!env.has_env()) return;
+            V3<T> vr{};
+            const int seen = escaped_light(P.cur.ray, vr);
+            if (seen == 0) return;
             P.throughput *= P.cur.transmittance;
             V3<T> eg = P.acc_grad * P.throughput;
             if (cfg.enable_mis && first) eg *= bmis;
             eg += P.acc_light_grad;
-            const V3<T> vr = background_bwd(P.cur.ray.d, eg, &P.cur.ray_dir_grad);
+            if (seen == 2) vr = background_bwd(P.cur.ray.d, eg, &P.cur.ray_dir_grad);
             P.cur.contribution = P.throughput * vr;
             if (cfg.enable_mis && first) P.cur.contribution *= bmis;
             P.cur.radiance += P.cur.contribution;
@@ -1215,6 +1516,13 @@ struct orc_scene {
     float min_transmittance;
     unsigned max_bounces;
     unsigned render_opts;
+    const float* lights;
+    const float* light_table;
+    const float* mesh_vertices;
+    const int* mesh_triangles;
+    const float* mesh_lights;
+    const float* mesh_tri_table;
+    int num_lights, light_entries, num_mesh_vertices, num_mesh_triangles, num_mesh_lights, mesh_tri_cols;
 };
 
 struct orc_fwd_out {
@@ -1262,6 +1570,14 @@ static Inputs to_in(const orc_scene* s) {
     in.min_transmittance = s->min_transmittance;
     in.max_bounces = s->max_bounces;
     in.render_opts = s->render_opts;
+    in.lights = s->lights; in.light_table = s->light_table; in.mesh_vertices = s->mesh_vertices;
+    in.mesh_triangles = s->mesh_triangles; in.mesh_lights = s->mesh_lights; in.mesh_tri_table = s->mesh_tri_table;
+    in.num_lights = s->lights ? s->num_lights : 0;
+    in.light_entries = s->light_table ? s->light_entries : 0;
+    in.num_mesh_vertices = s->mesh_vertices ? s->num_mesh_vertices : 0;
+    in.num_mesh_triangles = s->mesh_triangles ? s->num_mesh_triangles : 0;
+    in.num_mesh_lights = s->mesh_lights ? s->num_mesh_lights : 0;
+    in.mesh_tri_cols = s->mesh_tri_table ? s->mesh_tri_cols : 0;
     return in;
 }
 
@@ -1411,5 +1727,29 @@ unsigned long long orc_launch_seed(unsigned x, unsigned y, unsigned z, unsigned 
 }
 
 int orc_num_threads(void) { return omp_get_max_threads(); }
+
+// Light samples from positions pos [m,3], sample i drawn from the launch stream (i, 0, 0, frame):
+// out [m,9] = wi xyz, Li rgb, pdf, dist, type; eval_pdf [m] = the light sampler's pdf of the
+// sampled direction (lightSampler.cuh:340-406). FP64.
+int orc_light_samples(const orc_config* c, const orc_scene* sc, int m, const float* pos, double* out,
+                      double* eval_pdf) {
+    const Config cfg = to_cfg(c);
+    const Inputs in = to_in(sc);
+    Instances<double> I;
+    build_instances<double>(cfg, in, I);
+    Tracer<double> tr(cfg, in, I);
+    for (int i = 0; i < m; ++i) {
+        Sampler s;
+        s.init_launch(unsigned(i), 0u, 0u, in.frame);
+        const V3<double> p{pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+        const auto ls = tr.sample_light(p, s);
+        double* o = out + 9 * size_t(i);
+        o[0] = ls.wi.x; o[1] = ls.wi.y; o[2] = ls.wi.z;
+        o[3] = ls.Li.x; o[4] = ls.Li.y; o[5] = ls.Li.z;
+        o[6] = ls.pdf; o[7] = ls.dist; o[8] = double(ls.type);
+        eval_pdf[i] = ls.pdf > 0.0 ? tr.light_pdf(p, ls.wi) : 0.0;
+    }
+    return 0;
+}
 
 }  // extern "C"

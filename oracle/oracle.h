@@ -175,6 +175,16 @@ struct Inputs {
     float min_transmittance = 0.001f;
     uint32_t max_bounces = 3;
     uint32_t render_opts = 0;
+    // punctual and area lights (threedgptir_tracer/tracer.py:40-119 LightBuffers), row-major
+    const float* lights = nullptr;          // [num_lights, 9]: type, position xyz, radius, radiance rgb, two_sided
+    const float* light_table = nullptr;     // [5, light_entries]: prob, alias, type, index, selection pdf
+    const float* mesh_vertices = nullptr;   // [num_mesh_vertices, 3]
+    const int* mesh_triangles = nullptr;    // [num_mesh_triangles, 3]
+    const float* mesh_lights = nullptr;     // [num_mesh_lights, 8]: tri offset, tri count, vtx offset, vtx count,
+                                            //   radiance rgb, two_sided
+    const float* mesh_tri_table = nullptr;  // [3, mesh_tri_cols]: prob, local alias, area pdf
+    int num_lights = 0, light_entries = 0, num_mesh_vertices = 0, num_mesh_triangles = 0, num_mesh_lights = 0,
+        mesh_tri_cols = 0;
 };
 
 // per-sample forward outputs (optixTracer.cpp:931-944 shapes), all [nz,h,w,C] float

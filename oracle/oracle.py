@@ -53,6 +53,10 @@ class _Scene(C.Structure):
         ("min_transmittance", C.c_float),
         ("max_bounces", C.c_uint),
         ("render_opts", C.c_uint),
+        ("lights", _FP), ("light_table", _FP), ("mesh_vertices", _FP), ("mesh_triangles", C.POINTER(C.c_int)),
+        ("mesh_lights", _FP), ("mesh_tri_table", _FP),
+        ("num_lights", C.c_int), ("light_entries", C.c_int), ("num_mesh_vertices", C.c_int),
+        ("num_mesh_triangles", C.c_int), ("num_mesh_lights", C.c_int), ("mesh_tri_cols", C.c_int),
     ]
 
 
@@ -101,6 +105,7 @@ def lib():
         L.orc_launch_seed.argtypes = [C.c_uint, C.c_uint, C.c_uint, C.c_uint]
         L.orc_launch_seed.restype = C.c_ulonglong
         L.orc_num_threads.restype = C.c_int
+        L.orc_light_samples.argtypes = [P(_Config), P(_Scene), C.c_int, _FP, P(C.c_double), P(C.c_double)]
         _LIB = L
     return _LIB
 
@@ -186,6 +191,22 @@ def _scene(keep: _Keep, s: dict) -> _Scene:
     sc.min_transmittance = float(s.get("min_transmittance", 0.001))
     sc.max_bounces = int(s.get("max_bounces", 3))
     sc.render_opts = int(s.get("render_opts", 0))
+    # punctual and area lights (LightBuffers): 2-D row-major tables, absent or empty = none
+    tables = (("lights", "lights", "num_lights", 0), ("light_alias_table", "light_table", "light_entries", 1),
+              ("mesh_light_vertices", "mesh_vertices", "num_mesh_vertices", 0),
+              ("mesh_lights", "mesh_lights", "num_mesh_lights", 0),
+              ("mesh_light_triangle_alias_table", "mesh_tri_table", "mesh_tri_cols", 1))
+    for key, field, count, axis in tables:
+        a = g(key)
+        if a is not None and a.ndim == 2 and a.size > 0:
+            setattr(sc, field, _f(a))
+            setattr(sc, count, int(a.shape[axis]))
+    tris = s.get("mesh_light_triangles")
+    if tris is not None and np.asarray(tris).size > 0:
+        tris = np.ascontiguousarray(np.asarray(tris, dtype=np.int32))
+        keep.items.append(tris)
+        sc.mesh_triangles = tris.ctypes.data_as(C.POINTER(C.c_int))
+        sc.num_mesh_triangles = int(tris.shape[0])
     return sc
 
 
@@ -279,6 +300,23 @@ def sampler_stream(x: int, y: int, z: int, frame: int, count: int) -> np.ndarray
 
 def launch_seed(x: int, y: int, z: int, frame: int) -> int:
     return int(lib().orc_launch_seed(x, y, z, frame))
+
+
+def light_samples(cfg: OracleConfig, scene: dict, positions: np.ndarray, frame: int = 0):
+    """One light sample per position (sample i from launch stream (i, 0, 0, frame)). Returns
+    (wi [m,3], Li [m,3], pdf [m], dist [m], type [m] int, pdf of wi under the light sampler [m]), FP64."""
+    keep = _Keep()
+    sc = _scene(keep, scene)
+    sc.frame = int(frame)
+    pos = keep.f32(positions).reshape(-1, 3)
+    m = pos.shape[0]
+    out = np.zeros((m, 9), np.float64)
+    ev = np.zeros(m, np.float64)
+    P = C.POINTER(C.c_double)
+    c = cfg._c()
+    rc = lib().orc_light_samples(C.byref(c), C.byref(sc), m, _f(pos), out.ctypes.data_as(P), ev.ctypes.data_as(P))
+    assert rc == 0
+    return out[:, :3], out[:, 3:6], out[:, 6], out[:, 7], out[:, 8].astype(np.int64), ev
 
 
 def num_threads() -> int:

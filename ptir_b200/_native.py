@@ -79,7 +79,11 @@ class PtirTraceArgs(C.Structure):
         ("env_h", C.c_int32), ("env_w", C.c_int32),
         ("environment_alias", _FP),
         ("alias_h", C.c_int32), ("alias_w", C.c_int32),
+        ("lights", _FP), ("light_alias", _FP), ("mesh_light_vertices", _FP),
+        ("mesh_light_triangles", _FP), ("mesh_lights", _FP), ("mesh_light_alias", _FP),
         ("num_lights", C.c_int32), ("num_light_entries", C.c_int32), ("num_mesh_lights", C.c_int32),
+        ("num_mesh_light_vertices", C.c_int32), ("num_mesh_light_triangles", C.c_int32),
+        ("mesh_light_alias_cols", C.c_int32),
         ("sh_indirect", C.c_uint32),
         ("sph_eval_degree", C.c_int32),
         ("min_transmittance", C.c_float),

@@ -125,8 +125,14 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, in
         return fail(t, PTIR_EINVAL, "particle_shading_normal is required when normals are enabled");
     if (a->sph_eval_degree < 0 || a->sph_eval_degree > t->cfg.sph_degree || a->sph_eval_degree > 3)
         return fail(t, PTIR_EINVAL, "sph_eval_degree must lie in [0, min(3, sph_degree)]");
-    if (a->num_lights != 0 || a->num_light_entries != 0 || a->num_mesh_lights != 0)
-        return fail(t, PTIR_EINVAL, "point, sphere and mesh lights are not supported (environment lighting only)");
+    if (a->num_lights < 0 || a->num_light_entries < 0 || a->num_mesh_lights < 0 || a->num_mesh_light_vertices < 0 ||
+        a->num_mesh_light_triangles < 0 || a->mesh_light_alias_cols < 0)
+        return fail(t, PTIR_EINVAL, "negative light table size");
+    if ((a->num_lights > 0 && !a->lights) || (a->num_light_entries > 0 && !a->light_alias) ||
+        (a->num_mesh_lights > 0 && !a->mesh_lights) || (a->num_mesh_light_vertices > 0 && !a->mesh_light_vertices) ||
+        (a->num_mesh_light_triangles > 0 && !a->mesh_light_triangles) ||
+        (a->mesh_light_alias_cols > 0 && !a->mesh_light_alias))
+        return fail(t, PTIR_EINVAL, "a light table with a non-zero size has no data");
     if ((reinterpret_cast<uintptr_t>(a->particle_density) & 15u) != 0)
         return fail(t, PTIR_EINVAL, "particle_density must be 16-byte aligned");
     const bool env = a->environment != nullptr && a->env_h > 0 && a->env_w > 0;
@@ -160,6 +166,18 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, in
     p.env.cos_z = (float)std::cos((double)rot_z);
     p.env.sin_x = 0.0f;
     p.env.cos_x = 1.0f;
+    p.lights.lights = a->num_lights > 0 ? a->lights : nullptr;
+    p.lights.num_lights = a->num_lights;
+    p.lights.table = a->num_light_entries > 0 ? a->light_alias : nullptr;
+    p.lights.entries = a->num_light_entries;
+    p.lights.vertices = a->num_mesh_light_vertices > 0 ? a->mesh_light_vertices : nullptr;
+    p.lights.num_vertices = a->num_mesh_light_vertices;
+    p.lights.triangles = a->num_mesh_light_triangles > 0 ? a->mesh_light_triangles : nullptr;
+    p.lights.num_triangles = a->num_mesh_light_triangles;
+    p.lights.mesh = a->num_mesh_lights > 0 ? a->mesh_lights : nullptr;
+    p.lights.num_mesh = a->num_mesh_lights;
+    p.lights.tri_table = a->mesh_light_alias_cols > 0 ? a->mesh_light_alias : nullptr;
+    p.lights.tri_cols = a->mesh_light_alias_cols;
     p.ray_ori = a->ray_origin;
     p.ray_dir = a->ray_direction;
     long long offset = 0, tile0 = 0;

@@ -45,6 +45,20 @@ enum Flags : unsigned {
     kExactReplay = 32u,  // backward re-traversals include the segment's last composited Gaussian
 };
 
+// Punctual and area lights: the reference's LightBuffers (threedgptir_tracer/tracer.py:40-119),
+// read as the packed float tables lightSampler.cuh and meshLight.cuh index. Counts of 0 leave
+// the environment as the only light.
+struct LightView {
+    const float* lights;     // [num_lights, 9]: type, position / center xyz, radius, radiance rgb, two_sided
+    const float* table;      // [5, entries]: alias prob, alias entry, light type, light index, selection pdf
+    const float* vertices;   // [num_vertices, 3] mesh-light vertices
+    const int* triangles;    // [num_triangles, 3] global vertex indices
+    const float* mesh;       // [num_mesh, 8]: triangle offset, triangle count, vertex offset, vertex count,
+                             //   radiance rgb, two_sided
+    const float* tri_table;  // [3, tri_cols]: alias prob, alias (local to the mesh), area pdf
+    int num_lights, entries, num_vertices, num_triangles, num_mesh, tri_cols;
+};
+
 struct ParticleView {
     const float4* density;   // [n, 3] float4 = pos.xyz dns | quat wxyz | scale.xyz pad
     const float* material;   // [n, 5]
@@ -76,6 +90,7 @@ struct TraceParams {
     AccelView accel;
     ParticleView part;
     EnvView env;
+    LightView lights;
     const float* ray_ori;        // [z, h, w, 3]
     const float* ray_dir;
     ViewDesc views[kMaxViews];   // the launches of this trace (one for the reference's single launch)

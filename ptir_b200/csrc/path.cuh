@@ -3,6 +3,7 @@
 #pragma once
 
 #include "device_types.h"
+#include "lights.cuh"
 #include "pcg.cuh"
 #include "shading.cuh"
 #include "storage.cuh"
@@ -44,8 +45,9 @@ PTIR_DEV void segment_reset(Segment& s, float3 o, float3 d, float last_hit) {
 }
 
 struct Emitter {
-    float3 dir, contribution;
+    float3 dir, contribution, light;
     float light_pdf, scatter_pdf;
+    float tmax;  // shadow-ray end: short of a sampled point on a light, unbounded for the environment
 };
 
 struct PathState {
@@ -174,11 +176,11 @@ PTIR_DEV float3 sh_radiance(const TraceParams& P, unsigned id, float3 d) {
 // Stochastic shadow transmittance: occluded at the first hit whose alpha beats a draw
 // (pathTracer.cuh:130-214).
 template <class Ctx>
-PTIR_DEV bool shadow_occluded(const Ctx& C, float3 o, float3 d, Pcg32& rng) {
+PTIR_DEV bool shadow_occluded(const Ctx& C, float3 o, float3 d, float tmax, Pcg32& rng) {
     const TraceParams& P = C.P;
     const float2 clip = clip_scene(P, o, d);
     float start = fmaxf(0.0f, clip.x - 1e-9f);
-    const float end = fminf(kFarT, clip.y) + 1e-9f;
+    const float end = fminf(tmax, clip.y) + 1e-9f;
     if (start >= end) return false;
     float kt[Ctx::K];
     unsigned kid[Ctx::K];
@@ -217,25 +219,23 @@ PTIR_DEV void shading_frame(const Segment& s, float3& n, float3& wo, float3& alb
 }
 
 PTIR_DEV void emitter_clear(Emitter& em) {
-    em.contribution = f3(0.0f);
+    em.contribution = em.light = f3(0.0f);
     em.light_pdf = 0.0f;
     em.scatter_pdf = 0.0f;
     em.dir = f3(0.0f);
+    em.tmax = kFarT;
 }
 
-// Next-event estimation toward the environment (pathTracer.cuh:461-504), first half: light
-// sample, visibility-independent checks and BRDF. Fills the emitter as if unoccluded and
-// returns true when a shadow ray has to decide it (nee_shadow).
+// Next-event estimation (pathTracer.cuh:461-504), first half: light sample, visibility-independent
+// checks and BRDF. Fills the emitter as if unoccluded and returns true when a shadow ray has to
+// decide it (nee_shadow).
 template <class Ctx>
 PTIR_DEV bool nee_prepare(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
     const TraceParams& P = C.P;
     emitter_clear(ps.em);
-    float lpdf = 0.0f;
-    float3 wi = f3(0.0f), Li = f3(0.0f);
-    if (env_light_present(P.env)) {
-        wi = sample_env_direction(P.env, rng, lpdf);
-        Li = env_radiance(P.env, wi, C.ctr.env);
-    }
+    const LightSample ls = sample_light(P, s.pos, rng, C.ctr.env);
+    const float lpdf = ls.pdf;
+    const float3 wi = ls.wi, Li = ls.Li;
     if (lpdf <= 0.0f || all_zero(Li)) return false;
     if (dot(s.snrm, wi) <= 0.0f) return false;
     float3 n, wo, alb;
@@ -244,9 +244,12 @@ PTIR_DEV bool nee_prepare(const Ctx& C, PathState& ps, const Segment& s, Pcg32& 
     shading_frame(s, n, wo, alb, met, metallic_on);
     float spdf;
     const BrdfTerms bc = eval_brdf<false>(wo, n, alb, met, clamp_rough(s.rough), wi, metallic_on, spdf);
+    if (ls.type == kLightPoint) spdf = 0.0f;  // a delta light: no BRDF-side MIS weight
     ps.em.dir = wi;
+    ps.em.tmax = ls.dist < 1e19f ? fmaxf(0.0f, ls.dist - 2e-2f) : kFarT;
     ps.em.light_pdf = lpdf;
     ps.em.scatter_pdf = spdf;
+    ps.em.light = Li;
     ps.em.contribution = ps.throughput * bc.value * Li / fmaxf(lpdf, 1e-6f);
     return true;
 }
@@ -257,7 +260,7 @@ template <class Ctx>
 PTIR_DEV void nee_shadow(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
     ++C.ctr.segments;
     const float3 wi = ps.em.dir;
-    if (shadow_occluded(C, s.pos + wi * 2e-2f, wi, rng)) emitter_clear(ps.em);
+    if (shadow_occluded(C, s.pos + wi * 2e-2f, wi, ps.em.tmax, rng)) emitter_clear(ps.em);
 }
 
 template <class Ctx>
@@ -283,12 +286,23 @@ PTIR_DEV void sample_next(const Ctx& C, PathState& ps, Segment& s, Pcg32& rng) {
         return;
     }
     ps.throughput = nt;
+    const float lpdf = (P.flags & kMis) ? light_sampler_pdf(P, s.pos, next) : 0.0f;
     const float3 origin = s.pos + normalize_or_keep(next) * 2e-2f;
     segment_reset(s, origin, next, 0.0f);
     if (P.flags & kMis) {
         s.scatter_pdf = b.pdf;
-        s.light_pdf = env_pdf(P.env, next);
+        s.light_pdf = lpdf;
     }
+}
+
+// What an escaped segment sees (environment.cuh:599-634): with render.visualize_lights the
+// nearest sphere or mesh light along its ray, else the environment. 0: nothing, 1: a light
+// (radiance in vr), 2: the environment (looked up by the caller).
+template <class Ctx>
+PTIR_DEV int escaped_light(const Ctx& C, const Segment& s, float3& vr) {
+    const TraceParams& P = C.P;
+    if ((P.flags & kVisualizeLights) && visible_area_light(P.lights, s.o, s.d, vr)) return 1;
+    return env_present(P.env) ? 2 : 0;
 }
 
 // Radiance gathered at the end of a segment (environment.cuh:636-715)
@@ -311,8 +325,10 @@ PTIR_DEV void accumulate_light(const Ctx& C, PathState& ps, Segment& s) {
             ps.acc += contrib;
             ps.acc_indirect += contrib;
         } else if (s.escaped) {
-            if (!env_present(P.env)) return;
-            const float3 vr = env_radiance(P.env, s.d, C.ctr.env);
+            float3 vr;
+            const int seen = escaped_light(C, s, vr);
+            if (seen == 0) return;
+            if (seen == 2) vr = env_radiance(P.env, s.d, C.ctr.env);
             ps.throughput *= s.transmittance;
             s.light += vr;
             ps.acc_light += vr;
@@ -328,8 +344,10 @@ PTIR_DEV void accumulate_light(const Ctx& C, PathState& ps, Segment& s) {
         ps.acc_direct += nee;
     }
     if (s.escaped) {
-        if (!env_present(P.env)) return;
-        const float3 vr = env_radiance(P.env, s.d, C.ctr.env);
+        float3 vr;
+        const int seen = escaped_light(C, s, vr);
+        if (seen == 0) return;
+        if (seen == 2) vr = env_radiance(P.env, s.d, C.ctr.env);
         ps.throughput *= s.transmittance;
         s.light += vr;
         ps.acc_light += vr;
@@ -688,12 +706,14 @@ PTIR_DEV void accumulate_light_bwd(const Ctx& C, const BwdInputs& B, PathState& 
             if (mis && first) contrib *= bmis;
             ps.acc -= contrib;
         } else if (s.escaped) {
-            if (!env_present(P.env)) return;
+            float3 vr;
+            const int seen = escaped_light(C, s, vr);
+            if (seen == 0) return;
             ps.throughput *= s.transmittance;
             float3 eg = ps.acc_grad * ps.throughput;
             if (mis && first) eg *= bmis;
             eg += ps.acc_light_grad;
-            const float3 vr = env_radiance_bwd(C, B, s.d, eg, s.ray_dir_grad);
+            if (seen == 2) vr = env_radiance_bwd(C, B, s.d, eg, s.ray_dir_grad);
             float3 contrib = ps.throughput * vr;
             if (mis && first) contrib *= bmis;
             ps.acc -= contrib;
@@ -702,12 +722,14 @@ PTIR_DEV void accumulate_light_bwd(const Ctx& C, const BwdInputs& B, PathState& 
     }
     if (mis && first) ps.acc -= ps.em.contribution * lmis;
     if (s.escaped) {
-        if (!env_present(P.env)) return;
+        float3 vr;
+        const int seen = escaped_light(C, s, vr);
+        if (seen == 0) return;
         ps.throughput *= s.transmittance;
         float3 eg = ps.acc_grad * ps.throughput;
         if (mis && first) eg *= bmis;
         eg += ps.acc_light_grad;
-        const float3 vr = env_radiance_bwd(C, B, s.d, eg, s.ray_dir_grad);
+        if (seen == 2) vr = env_radiance_bwd(C, B, s.d, eg, s.ray_dir_grad);
         float3 contrib = ps.throughput * vr;
         if (mis && first) contrib *= bmis;
         s.radiance += contrib;
@@ -726,7 +748,10 @@ PTIR_DEV void pending_bwd(PathState& ps, const Segment& s, Replay&& replay) {
                      ps.pend_bounces > 1u ? 1u : 0u});
 }
 
-// pathTracer.cuh:506-548 (albedo only; the environment and roughness terms are disabled there)
+// pathTracer.cuh:506-548 (albedo only; the environment and roughness terms are disabled there).
+// The reference weights the term by the environment's radiance in the sampled direction, whatever
+// light was sampled; with exact_replay the sampled light's radiance is used, which is the same
+// for environment samples and the derivative of the estimator for the other lights.
 template <class Ctx>
 PTIR_DEV void nee_grad_bwd(const Ctx& C, PathState& ps, Segment& s, const Segment& it) {
     const TraceParams& P = C.P;
@@ -738,7 +763,7 @@ PTIR_DEV void nee_grad_bwd(const Ctx& C, PathState& ps, Segment& s, const Segmen
     float spdf;
     const BrdfTerms g = eval_brdf<true>(wo, n, alb, met, it.rough, ps.em.dir, metallic_on, spdf);
     const float scale = mis_weight(ps.em.light_pdf, ps.em.scatter_pdf) / fmaxf(ps.em.light_pdf, 1e-6f);
-    const float3 bgc = env_radiance(P.env, ps.em.dir, C.ctr.env);
+    const float3 bgc = (P.flags & kExactReplay) ? ps.em.light : env_radiance(P.env, ps.em.dir, C.ctr.env);
     const float3 dl = ps.acc_grad * ps.throughput * bgc * scale;
     s.d_albedo += dl * g.d_albedo;
 }
@@ -765,7 +790,7 @@ PTIR_DEV void sample_next_bwd(const Ctx& C, PathState& ps, Segment& s, Pcg32& rn
     float lpdf = 0.0f;
     bool first_nee = false;
     if (mis) {
-        lpdf = env_pdf(P.env, next);
+        lpdf = light_sampler_pdf(P, it.pos, next);
         first_nee = ps.bounces == 1u && max3(nt) >= 1e-4f;
         if (first_nee) nee_grad_bwd(C, ps, s, it);
     }

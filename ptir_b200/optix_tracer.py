@@ -34,6 +34,31 @@ def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
 
+def _light_tables(lights, light_alias_table, mesh_light_vertices, mesh_light_triangles, mesh_lights,
+                  mesh_light_triangle_alias_table) -> list:
+    """The six LightBuffers tensors (threedgptir_tracer/tracer.py:40-119) as contiguous CUDA tensors,
+    None where a table is absent or empty; shapes are checked as the kernels index them."""
+    specs = ((lights, "lights", 9, None, torch.float32), (light_alias_table, "light_alias_table", None, 5, torch.float32),
+             (mesh_light_vertices, "mesh_light_vertices", 3, None, torch.float32),
+             (mesh_light_triangles, "mesh_light_triangles", 3, None, torch.int32),
+             (mesh_lights, "mesh_lights", 8, None, torch.float32),
+             (mesh_light_triangle_alias_table, "mesh_light_triangle_alias_table", None, 3, torch.float32))
+    out = []
+    for t, name, cols, rows, dtype in specs:
+        if t is None or t.numel() == 0:
+            out.append(None)
+            continue
+        if t.dim() != 2 or (cols is not None and t.shape[1] != cols) or (rows is not None and t.shape[0] != rows):
+            shape = f"[{rows}, K]" if rows is not None else f"[K, {cols}]"
+            raise ValueError(f"{name} must be {shape}, got {tuple(t.shape)}")
+        if t.dtype != dtype:
+            raise TypeError(f"{name}: unsupported dtype {t.dtype} ({dtype} required)")
+        if not t.is_cuda:
+            raise ValueError(f"{name}: CUDA tensor required")
+        out.append(t.contiguous())
+    return out
+
+
 def split_views(flat: torch.Tensor, views) -> list:
     """Per-view [Z,H,W,C...] views of a flat per-sample tensor [T,C...] of trace_views()."""
     out, start = [], 0
@@ -164,10 +189,9 @@ class OptixTracer:
         alias_ok = (isinstance(alias, torch.Tensor) and alias.dim() == 3 and alias.shape[0] == 3 and alias.shape[1] > 0
                     and alias.shape[2] > 0)
         alias = _f32(alias, "environment_alias_table") if alias_ok else None
-        n_lights = int(lights.shape[0]) if lights is not None else 0
-        n_entries = int(light_alias_table.shape[1]) if light_alias_table is not None and light_alias_table.dim() == 2 else 0
-        n_mesh = int(mesh_lights.shape[0]) if mesh_lights is not None else 0
-        keep += [t2w, ori, dirs, dens, mat, rad, snrm, env, alias]
+        lt = _light_tables(lights, light_alias_table, mesh_light_vertices, mesh_light_triangles, mesh_lights,
+                           mesh_light_triangle_alias_table)
+        keep += [t2w, ori, dirs, dens, mat, rad, snrm, env, alias, *lt]
         a = N.PtirTraceArgs()
         a.frame = int(frame) & 0xFFFFFFFF
         a.ray_to_world = _ptr(t2w)
@@ -180,7 +204,15 @@ class OptixTracer:
         a.env_h, a.env_w = (int(env.shape[0]), int(env.shape[1])) if env is not None else (0, 0)
         a.environment_alias = _ptr(alias)
         a.alias_h, a.alias_w = (int(alias.shape[1]), int(alias.shape[2])) if alias is not None else (0, 0)
-        a.num_lights, a.num_light_entries, a.num_mesh_lights = n_lights, n_entries, n_mesh
+        lgt, table, verts, tris, mesh, tri_table = lt
+        a.lights, a.light_alias, a.mesh_light_vertices = _ptr(lgt), _ptr(table), _ptr(verts)
+        a.mesh_light_triangles, a.mesh_lights, a.mesh_light_alias = _ptr(tris), _ptr(mesh), _ptr(tri_table)
+        a.num_lights = int(lgt.shape[0]) if lgt is not None else 0
+        a.num_light_entries = int(table.shape[1]) if table is not None else 0
+        a.num_mesh_light_vertices = int(verts.shape[0]) if verts is not None else 0
+        a.num_mesh_light_triangles = int(tris.shape[0]) if tris is not None else 0
+        a.num_mesh_lights = int(mesh.shape[0]) if mesh is not None else 0
+        a.mesh_light_alias_cols = int(tri_table.shape[1]) if tri_table is not None else 0
         a.sh_indirect = int(sh_indirect)
         a.sph_eval_degree = int(sph_degree)
         a.min_transmittance = float(min_transmittance)

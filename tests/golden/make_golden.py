@@ -5,6 +5,9 @@
   alias_tables.npz   environment importance tables from the reference's own
                      threedgrut/model/aliastable.py on seeded environments
   oracle_small.npz   FP64 oracle render of a tiny seeded scene (pins the oracle against regressions)
+  light_tables.npz   packed point / sphere / mesh light tables and top-level light alias tables
+                     from the reference's own threedgrut/model/light.py (its image-loading import,
+                     imageio, is absent here and unused by these functions, so it is stubbed)
 
 Usage: python tests/golden/make_golden.py [--reference /root/reference]
 """
@@ -64,6 +67,72 @@ def alias_tables(reference):
     np.savez_compressed(os.path.join(HERE, "alias_tables.npz"), **arrays)
 
 
+def light_case(name):
+    """Light descriptions and environment of a light-table case (regenerated by the tests)."""
+    from ptir_b200 import synthetic
+
+    quad = dict(type="mesh", vertices=[[-0.5, 2.0, -0.5], [0.5, 2.0, -0.5], [0.5, 2.0, 0.5], [-0.5, 2.0, 0.5]],
+                triangles=[[0, 1, 2], [0, 2, 3]], radiance=(4.0, 3.5, 3.0), two_sided=False)
+    strip = dict(type="mesh", vertices=[[1.0, -1.0, 0.0], [1.5, -1.0, 0.2], [1.2, -0.4, 0.1], [1.9, -0.5, 0.4],
+                                        [1.2, -0.4, 0.1]],
+                 triangles=[[0, 1, 2], [1, 3, 2], [2, 2, 4]], radiance=(0.5, 1.0, 2.0), two_sided=True)
+    if name == "mixed":
+        lights = [dict(type="point", position=(0.3, 1.5, -0.2), intensity=(2.0, 1.5, 1.0)),
+                  dict(type="sphere", center=(-1.0, 1.2, 0.5), radius=0.25, radiance=(3.0, 3.0, 2.5)),
+                  dict(type="point", position=(-0.4, -1.1, 0.9), intensity=(0.0, 0.0, 0.0)),
+                  dict(type="sphere", center=(0.8, 0.9, 1.3), radius=0.1, radiance=(10.0, 2.0, 1.0), two_sided=True),
+                  quad, strip]
+        return lights, synthetic.make_environment(32, 64, seed=11), "2d"
+    if name == "point_only":
+        return [dict(type="point", position=(0.0, 2.0, 0.0), intensity=(5.0, 5.0, 5.0))], None, "2d"
+    if name == "cube_sphere":
+        return ([dict(type="sphere", center=(0.0, 0.0, 3.0), radius=0.5, radiance=(1.0, 0.5, 0.25))],
+                synthetic.make_environment(48, 8, seed=12), "cube")
+    raise KeyError(name)
+
+
+LIGHT_CASES = ("mixed", "point_only", "cube_sphere")
+
+
+def _reference_light_module(reference):
+    import types
+
+    for m in ("imageio", "imageio.plugins", "imageio.plugins.freeimage"):
+        if m not in sys.modules:
+            mod = types.ModuleType(m)
+            mod.__path__ = []
+            sys.modules[m] = mod
+    sys.modules["imageio"].plugins = sys.modules["imageio.plugins"]
+    sys.modules["imageio.plugins"].freeimage = sys.modules["imageio.plugins.freeimage"]
+    sys.path.insert(0, reference)
+    import threedgrut.model.light as L  # noqa: E402
+
+    return L
+
+
+def light_tables(reference):
+    import torch
+
+    L = _reference_light_module(reference)
+    arrays = {}
+    for name in LIGHT_CASES:
+        lights, env, kind = light_case(name)
+        analytic = [L.Light.from_dict(d) for d in lights if d["type"] != "mesh"]
+        meshes = [L.Light.from_dict(d) for d in lights if d["type"] == "mesh"]
+        packed = L.Light.pack_lights(analytic, dtype=torch.float32)
+        pack = L.pack_mesh_lights(meshes, dtype=torch.float32)
+        table = L.build_light_alias_table(environment=None if env is None else torch.as_tensor(env),
+                                          environment_type=kind, lights=packed, mesh_powers=pack.powers)
+        arrays[f"{name}_lights"] = packed.numpy()
+        arrays[f"{name}_table"] = (np.zeros((5, 0), np.float32) if table is None else table.pack().numpy())
+        arrays[f"{name}_mesh_vertices"] = pack.vertices.numpy()
+        arrays[f"{name}_mesh_triangles"] = pack.triangles.numpy()
+        arrays[f"{name}_mesh_lights"] = pack.params.numpy()
+        arrays[f"{name}_mesh_tri_table"] = pack.triangle_alias_table.numpy()
+        arrays[f"{name}_mesh_powers"] = pack.powers.numpy()
+    np.savez_compressed(os.path.join(HERE, "light_tables.npz"), **arrays)
+
+
 def oracle_small():
     from oracle import oracle as O
     from tests.scenes import small_scene
@@ -87,5 +156,6 @@ if __name__ == "__main__":
     a = ap.parse_args()
     sampler_kat(a.reference)
     alias_tables(a.reference)
+    light_tables(a.reference)
     oracle_small()
     print("golden fixtures written to", HERE)

@@ -42,6 +42,36 @@ def small_scene(n=2000, w=48, h=40, spp=1, views=1, max_bounces=3, env_hw=(32, 6
     return s
 
 
+LIGHT_KEYS = ("lights", "light_alias_table", "mesh_light_vertices", "mesh_light_triangles", "mesh_lights",
+              "mesh_light_triangle_alias_table")
+
+
+def with_lights(s: dict, lights, environment=True) -> dict:
+    """The scene with the packed tables of `lights` (point / sphere / mesh dicts) and a top-level
+    light table that includes the scene's environment when `environment` is set and it has one."""
+    from ptir_b200.lights import light_buffers
+
+    env = s.get("environment")
+    env_t = torch.from_numpy(env) if environment and env is not None and env.size > 0 else None
+    lb = light_buffers(lights, environment=env_t)
+    tables = dict(zip(LIGHT_KEYS, (t.numpy() for t in lb.tensors())))
+    return dict(s, **tables)
+
+
+def _light_tensors(S: dict) -> tuple:
+    dev = S["density"].device
+    empty = {"lights": (0, 9), "light_alias_table": (5, 0), "mesh_light_vertices": (0, 3),
+             "mesh_light_triangles": (0, 3), "mesh_lights": (0, 8), "mesh_light_triangle_alias_table": (3, 0)}
+    out = []
+    for k in LIGHT_KEYS:
+        if k in S:
+            out.append(S[k])
+        else:
+            dt = torch.int32 if k == "mesh_light_triangles" else torch.float32
+            out.append(torch.empty(empty[k], dtype=dt, device=dev))
+    return tuple(out)
+
+
 def to_torch(s: dict, device="cuda") -> dict:
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(device)  # noqa: E731
     return {k: (t(v) if isinstance(v, np.ndarray) else v) for k, v in s.items()}
@@ -80,17 +110,14 @@ def round_scene(s: dict, storage: str) -> dict:
 
 def gpu_trace(tr, S: dict, build=True, rebuild=True):
     """Run build_bvh + trace on torch CUDA scene S (from to_torch). Returns the 13-tuple."""
-    empty = lambda *shape, dt=torch.float32: torch.empty(shape, dtype=dt, device=S["density"].device)  # noqa: E731
     if build:
         tr.build_bvh(S["build_pos"], S["build_rot"], S["build_scl"], S["build_dns"], rebuild, True)
     return tr.trace(S["frame"], S["ray_to_world"], S["ray_ori"], S["ray_dir"], S["density"], S["material"], S["sph"],
-                    S["shading_normal"], S["environment"], S["alias_table"], empty(0, 9), empty(5, 0), empty(0, 3),
-                    empty(0, 3, dt=torch.int32), empty(0, 8), empty(3, 0), S["render_opts"], S["sph_degree"],
-                    S["min_transmittance"], S["max_bounces"])
+                    S["shading_normal"], S["environment"], S["alias_table"], *_light_tensors(S), S["render_opts"],
+                    S["sph_degree"], S["min_transmittance"], S["max_bounces"])
 
 
 def gpu_trace_bwd(tr, S: dict, fwd, pbr_grad, light_grad=None, material_grad=None):
-    empty = lambda *shape, dt=torch.float32: torch.empty(shape, dtype=dt, device=S["density"].device)  # noqa: E731
     (rad, dns, hit, hit2, dist, nrm, snrm, mat, hits, vis, pbr, light, comps) = fwd
     z = lambda t: torch.zeros_like(t)  # noqa: E731
     if light_grad is None:
@@ -99,7 +126,6 @@ def gpu_trace_bwd(tr, S: dict, fwd, pbr_grad, light_grad=None, material_grad=Non
         material_grad = z(mat)
     return tr.trace_bwd(S["frame"], S["ray_to_world"], S["ray_ori"], S["ray_dir"], rad, dns, hit, hit2, dist, nrm, snrm,
                         mat, pbr, light, S["density"], S["material"], S["sph"], S["shading_normal"], S["environment"],
-                        S["alias_table"], empty(0, 9), empty(5, 0), empty(0, 3), empty(0, 3, dt=torch.int32),
-                        empty(0, 8), empty(3, 0), z(rad), z(dns), z(hit), z(hit2), z(dist), z(nrm), z(snrm),
+                        S["alias_table"], *_light_tensors(S), z(rad), z(dns), z(hit), z(hit2), z(dist), z(nrm), z(snrm),
                         material_grad, pbr_grad, light_grad, S["render_opts"], S["sph_degree"], S["min_transmittance"],
                         S["max_bounces"])
