@@ -16,6 +16,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
+from ptir_b200 import synthetic
 from tests.golden.make_golden import light_case
 from tests.scenes import gpu_trace, gpu_trace_bwd, make_tracer, small_scene, to_torch, with_lights
 
@@ -122,8 +123,11 @@ def test_backward_with_lights(cuda_device, case, schedule):
 
 
 def test_point_light_albedo_gradient_matches_central_differences(cuda_device):
+    # the light sits between the camera and the field, so that surfaces the camera sees are lit
+    eye = synthetic.camera_positions(1, seed=0)[0]
+    light = dict(type="point", position=tuple(0.7 * eye + np.array([0.3, 0.2, 0.1])), intensity=(6.0, 5.0, 4.0))
     s = with_lights(small_scene(n=1500, w=32, h=24, spp=2, max_bounces=2, scale_range=(0.03, 0.12), env=False),
-                    [dict(type="point", position=(0.2, 2.0, 0.3), intensity=(6.0, 5.0, 4.0))], environment=False)
+                    [light], environment=False)
     rng = np.random.default_rng(8)
     W = rng.standard_normal(s["ray_ori"].shape[:3] + (3,)).astype(np.float32)
     ref, vis, _ = O.trace(O.OracleConfig(), s, "f64")
