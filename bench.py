@@ -300,6 +300,8 @@ def run_ours(args, rank, world, device):
     shape = {}
     if not args.no_autotune:
         shape = tune_launch_shape(S, args, device)
+    if args.kbuffer:
+        shape = dict(shape, kbuffer=args.kbuffer)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     # target image: the same scene with albedo perturbed by N(0, 0.02)
@@ -570,6 +572,8 @@ def main():
     ap.add_argument("--storage", default="bf16", choices=("fp32", "bf16", "fp16"),
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kbuffer", type=int, default=0, choices=(0, 8, 16, 24, 32),
+                    help="candidates per traversal (0: the tuned or default size)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

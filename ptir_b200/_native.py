@@ -120,15 +120,17 @@ EXPORTS = ("ptir_abi_version", "ptir_create", "ptir_destroy", "ptir_build_bvh", 
 
 
 def lib_path() -> str:
-    return _build.LIB_PATH
+    """The library loaded: $PTIR_B200_LIBRARY when set (a build kept elsewhere, loaded as it is),
+    else the in-tree build."""
+    return os.environ.get("PTIR_B200_LIBRARY") or _build.LIB_PATH
 
 
 def load(build_if_missing: bool = True):
-    """Load the shared library (building it first when it is missing or stale)."""
+    """Load the shared library (building the in-tree one first when it is missing or stale)."""
     global _LIB
     if _LIB is not None:
         return _LIB
-    if build_if_missing and _build.needs_build():
+    if build_if_missing and not os.environ.get("PTIR_B200_LIBRARY") and _build.needs_build():
         _build.build()
     path = lib_path()
     if not os.path.exists(path):

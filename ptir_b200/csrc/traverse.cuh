@@ -180,11 +180,16 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, const TraceState& t, 
     v.ch[3] = __float_as_int(cc.w);
     v.hits = 0;
     unsigned leaves = 0;
+    // plane distance (p - o) / d as one FMA, p * inv - o * inv. A NaN (0 * inf, or inf - inf for a
+    // ray parallel to an axis) leaves the axis unbounded, so the test stays conservative.
+    const float3 oi = make_float3(o.x * inv.x, o.y * inv.y, o.z * inv.z);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        // clipped slab interval [a, b]; a NaN plane distance (0 * inf) leaves its axis unbounded
-        const float a = max3f((nxa[k] - o.x) * inv.x, (nya[k] - o.y) * inv.y, fmaxf((nza[k] - o.z) * inv.z, tmin));
-        const float b = min3f((fxa[k] - o.x) * inv.x, (fya[k] - o.y) * inv.y, fminf((fza[k] - o.z) * inv.z, tend));
+        // clipped slab interval [a, b]
+        const float a = max3f(fmaf(nxa[k], inv.x, -oi.x), fmaf(nya[k], inv.y, -oi.y),
+                              fmaxf(fmaf(nza[k], inv.z, -oi.z), tmin));
+        const float b = min3f(fmaf(fxa[k], inv.x, -oi.x), fmaf(fya[k], inv.y, -oi.y),
+                              fminf(fmaf(fza[k], inv.z, -oi.z), tend));
         v.t0[k] = a;
         // nearer middle of the clipped interval first: boxes that contain the origin all
         // enter at tmin, their extent along the ray tells them apart
@@ -198,7 +203,7 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, const TraceState& t, 
 
 // Descent after the leaf tests: into the nearest internal child still in front of the K-th
 // distance, the others pushed farthest first; else the next stacked subtree that can still hold
-// a nearer candidate. Returns false when the call is complete.
+// a nearer candidate. Returns false when no node visit remains.
 template <int K>
 PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], int* stack, float* stack_t,
                       unsigned* err, TraceCounters& ctr) {
@@ -221,7 +226,6 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
         const int np = __popc(inner);
         if (sp + np > kStackDepth) {
             atomicOr(err, kErrStackOverflow);
-            ctr.candidates += kbuf_count(kt);
             return false;
         }
         while (inner) {
@@ -252,10 +256,7 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
                 break;
             }
         }
-        if (!found) {
-            ctr.candidates += kbuf_count(kt);
-            return false;
-        }
+        if (!found) return false;
     }
     t.sp = sp;
     t.node = node;
@@ -277,7 +278,9 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
         ++ctr.leaves;
         test_leaf(A, ~c, o, d, t.tmin, t.tend, kt, kid);
     }
-    return descend(t, v, kt, stack, stack_t, err, ctr);
+    if (descend(t, v, kt, stack, stack_t, err, ctr)) return true;
+    ctr.candidates += kbuf_count(kt);
+    return false;
 }
 
 // Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
