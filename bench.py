@@ -302,6 +302,8 @@ def run_ours(args, rank, world, device):
         shape = tune_launch_shape(S, args, device)
     if args.kbuffer:
         shape = dict(shape, kbuffer=args.kbuffer)
+    if args.no_warp_aggregate:
+        shape = dict(shape, warp_aggregate=False)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     # target image: the same scene with albedo perturbed by N(0, 0.02)
@@ -554,6 +556,78 @@ def cpu_sample(args, S=None, threads=0, budget_s=15.0):
                       f"fwd+bwd oracle FP32, {dt:.1f} s", "seconds": dt, "segments": segs}
 
 
+def accuracy_sample(args, shape: dict, device, name: str = "field-300k-sh", res=(128, 96)) -> dict:
+    """Image and gradient error of the tracer (the run's launch shape) against the FP64 oracle fed
+    the same per-path sample sequences, for each attribute storage: config 4 of the benchmark (the
+    300k-Gaussian scene with degree-3 SH, 512x1024 environment, 3 bounces) on one view of res at
+    1 spp, since the full view is beyond the oracle's reach. (The timed 1M-Gaussian scene is no use
+    here: its background shell is opaque, so no light reaches the camera and its PBR image is
+    black.) With 16-bit storage the oracle gets the attributes rounded as the tracer holds them.
+    Both backward passes start from the oracle's forward values with the same seeded pbr
+    gradient."""
+    from oracle import oracle as O
+
+    wl = synthetic.workload(name)
+    f = synthetic.make_field(wl.n, seed=wl.seed, layout=wl.layout, scale_range=wl.scale_range, sh_full=wl.sh_full)
+    env = synthetic.make_environment(*wl.env_hw, seed=wl.seed)
+    alias = envmap.pack(envmap.build(env))
+    w, h = res
+    o, d = synthetic.pinhole_rays(w, h, synthetic.camera_positions(1, seed=wl.seed)[0])
+    attrs = dict(build_pos=f["pos"], build_rot=f["rot"], build_scl=f["scl"], build_dns=f["dns"],
+                 density=synthetic.density_tensor(f), material=synthetic.material_tensor(f), sph=f["sph"],
+                 shading_normal=f["snrm"])
+    g = np.random.default_rng(7).standard_normal((1, h, w, 3)).astype(np.float32) / float(h * w)
+    dev = lambda t: t.to(device).contiguous()  # noqa: E731
+    ori, drs = dev(torch.from_numpy(o[None].astype(np.float32))), dev(torch.from_numpy(d[None].astype(np.float32)))
+    e_env, e_alias, t2w = dev(env), dev(alias), torch.eye(4, device=device).reshape(1, 4, 4)
+    e = lambda *sh, dt=torch.float32: torch.empty(sh, dtype=dt, device=device)  # noqa: E731
+    lights = (e(0, 9), e(5, 0), e(0, 3), e(0, 3, dt=torch.int32), e(0, 8), e(3, 0))
+
+    def rel_cos(a, b):
+        a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+        nb = max(np.linalg.norm(b), 1e-30)
+        return float(np.linalg.norm(a - b) / nb), float(a @ b / max(np.linalg.norm(a) * nb, 1e-30))
+
+    out = {"reference": "FP64 oracle, same sample sequences",
+           "sample": f"{wl.name} (config 4 scene): 1 view {w}x{h} at 1 spp, {wl.max_bounces} bounces"}
+    t0 = time.perf_counter()
+    for storage, rnd in (("fp32", None), ("bf16", torch.bfloat16), ("fp16", torch.float16)):
+        held = {k: (t if rnd is None else t.to(rnd).float()) for k, t in attrs.items()}
+        scene = dict({k: t.numpy() for k, t in held.items()}, environment=env.numpy(), alias_table=alias.numpy(),
+                     ray_to_world=np.eye(4, dtype=np.float32)[None], frame=0, sph_degree=3, min_transmittance=0.001,
+                     max_bounces=wl.max_bounces, ray_ori=o[None].astype(np.float32), ray_dir=d[None].astype(np.float32))
+        cfg = O.OracleConfig()
+        ref, _, _ = O.trace(cfg, scene, "f64")
+        mg_ref, eg_ref, _ = O.trace_bwd(cfg, scene, ref, dict(pbr=g), "f64")
+        from ptir_b200 import OptixTracer
+
+        tr = OptixTracer("", "", "reference", "referenceBwd", "instances", 4, 0.0113, True, 3, True, True, True,
+                         False, False, storage=storage, **shape)
+        tr.build_bvh(dev(f["pos"]), dev(f["rot"]), dev(f["scl"]), dev(f["dns"]), True, True)
+        scene_t = (dev(attrs["density"]), dev(attrs["material"]), dev(f["sph"]), dev(f["snrm"]), e_env, e_alias,
+                   *lights)
+        fwd = list(tr.trace(0, t2w, ori, drs, *scene_t, 0, 3, 0.001, wl.max_bounces))
+        pbr = fwd[10].cpu().numpy()
+        fwd[10] = torch.from_numpy(ref["pbr"]).to(device)
+        fwd[11] = torch.from_numpy(ref["light"]).to(device)
+        z = torch.zeros_like
+        bw = tr.trace_bwd(0, t2w, ori, drs, *fwd[:8], fwd[10], fwd[11], *scene_t, z(fwd[0]), z(fwd[1]), z(fwd[2]),
+                          z(fwd[3]), z(fwd[4]), z(fwd[5]), z(fwd[6]), z(fwd[7]), torch.from_numpy(g).to(device),
+                          z(fwd[11]), 0, 3, 0.001, wl.max_bounces)
+        mg, eg = bw[1].cpu().numpy(), bw[4].cpu().numpy()
+        err = np.abs(pbr.astype(np.float64) - ref["pbr"].astype(np.float64))
+        ok = np.all(err <= 1e-3 + 1e-3 * np.abs(ref["pbr"]), axis=-1)
+        m_rel, m_cos = rel_cos(mg[:, :4], mg_ref[:, :4])
+        e_rel, e_cos = rel_cos(eg[..., :3], eg_ref[..., :3])
+        out[storage] = {"pbr_within_1e-3": round(float(ok.mean()), 5), "pbr_max_abs": float(err.max()),
+                        "pbr_mean_abs": float(err.mean()), "pbr_rel_l2": rel_cos(pbr, ref["pbr"])[0],
+                        "material_grad_rel_l2": m_rel, "material_grad_cos": m_cos,
+                        "env_grad_rel_l2": e_rel, "env_grad_cos": e_cos}
+        del tr
+    out["seconds"] = round(time.perf_counter() - t0, 1)
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -572,6 +646,9 @@ def main():
     ap.add_argument("--storage", default="bf16", choices=("fp32", "bf16", "fp16"),
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the error report against the FP64 oracle")
+    ap.add_argument("--no-warp-aggregate", action="store_true",
+                    help="one gradient atomic per lane and term (default: warp-aggregated rows)")
     ap.add_argument("--kbuffer", type=int, default=0, choices=(0, 8, 16, 24, 32),
                     help="candidates per traversal (0: the tuned or default size)")
     args = ap.parse_args()
@@ -622,6 +699,9 @@ def main():
         if world == 1 and not args.no_cpu_baseline:
             cb = cpu_sample(args, S)
             res["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if world == 1 and not args.no_accuracy:
+            shape = res["config"]["launch"] if isinstance(res["config"].get("launch"), dict) else {}
+            res["accuracy"] = accuracy_sample(args, shape, device)
         print(json.dumps(res))
 
 

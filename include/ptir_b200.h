@@ -85,6 +85,9 @@ typedef struct ptir_config {
                                      they are), _BF16 or _FP16 (geometry, material, shading normal and SH
                                      rounded to nearest even once per call and by build_bvh; arithmetic
                                      stays FP32) */
+    int32_t grad_aggregate;       /* gradient scatter: 0 = lanes of a warp that add to the same Gaussian or
+                                     texel sum their terms first and one of them issues the atomics
+                                     (default), 1 = one atomic per lane and term as the reference */
 } ptir_config;
 
 enum { PTIR_STORAGE_FP32 = 0, PTIR_STORAGE_BF16 = 1, PTIR_STORAGE_FP16 = 2 };

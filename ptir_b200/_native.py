@@ -42,6 +42,7 @@ class PtirConfig(C.Structure):
         ("exact_replay", C.c_int32),
         ("grad_sums", C.c_int32),
         ("storage", C.c_int32),
+        ("grad_aggregate", C.c_int32),
     ]
 
 

@@ -80,6 +80,7 @@ unsigned flags_of(const ptir_config& c) {
     if (c.enable_metallic) f |= ptir::kMetallic;
     if (c.visualize_lights) f |= ptir::kVisualizeLights;
     if (c.exact_replay) f |= ptir::kExactReplay;
+    if (c.grad_aggregate == 0) f |= ptir::kWarpAggregate;
     return f;
 }
 
@@ -278,6 +279,7 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
         return PTIR_EINVAL;
     if (config->ray_order != 0 && config->ray_order != 1) return PTIR_EINVAL;
     if (config->grad_sums != 0 && config->grad_sums != 1) return PTIR_EINVAL;
+    if (config->grad_aggregate != 0 && config->grad_aggregate != 1) return PTIR_EINVAL;
     if (config->storage != PTIR_STORAGE_FP32 && config->storage != PTIR_STORAGE_BF16 &&
         config->storage != PTIR_STORAGE_FP16)
         return PTIR_EINVAL;

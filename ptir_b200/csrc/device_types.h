@@ -43,6 +43,7 @@ enum Flags : unsigned {
     kMetallic = 8u,
     kVisualizeLights = 16u,
     kExactReplay = 32u,  // backward re-traversals include the segment's last composited Gaussian
+    kWarpAggregate = 64u,  // gradient rows shared by lanes of a warp are summed before the atomics
 };
 
 // Punctual and area lights: the reference's LightBuffers (threedgptir_tracer/tracer.py:40-119),

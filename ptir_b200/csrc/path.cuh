@@ -582,6 +582,49 @@ PTIR_DEV void grad_add(float* g, float* comp, float v) {
     if (err != 0.0f) atomicAdd(comp, err);
 }
 
+// Scatter of one row of gradient terms (a Gaussian's material row, an environment texel's
+// colour), terms v[0..n). With kWarpAggregate the active lanes that add to the same row first
+// combine their terms, by shuffles in lane order, and the lowest of them issues the row's
+// atomics: the atomic traffic on a popular Gaussian or texel falls by the number of lanes that
+// share it, and only the order of the float additions changes. With a compensation buffer the
+// rounding errors of that combination (TwoSum) go to the buffer too, so the compensated sums
+// keep their accuracy whichever lanes happen to meet.
+template <int N>
+PTIR_DEV void grad_add_row(unsigned flags, float* g, float* comp, float (&v)[N], int n) {
+    float err[N];
+#pragma unroll
+    for (int k = 0; k < N; ++k) err[k] = 0.0f;
+    if (flags & kWarpAggregate) {
+        const unsigned lane = threadIdx.x & 31u;
+        const unsigned peers = __match_any_sync(__activemask(), reinterpret_cast<unsigned long long>(g));
+        if (peers != (1u << lane)) {
+            float sum[N];
+#pragma unroll
+            for (int k = 0; k < N; ++k) sum[k] = 0.0f;
+            for (unsigned m = peers; m; m &= m - 1u) {
+                const int src = __ffs(m) - 1;
+#pragma unroll
+                for (int k = 0; k < N; ++k) {
+                    const float x = __shfl_sync(peers, v[k], src);
+                    const float t = __fadd_rn(sum[k], x);
+                    const float bp = __fsub_rn(t, sum[k]);
+                    err[k] = __fadd_rn(err[k], __fadd_rn(__fsub_rn(sum[k], __fsub_rn(t, bp)), __fsub_rn(x, bp)));
+                    sum[k] = t;
+                }
+            }
+            if ((int)lane != __ffs(peers) - 1) return;
+#pragma unroll
+            for (int k = 0; k < N; ++k) v[k] = sum[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        if (k >= n) continue;
+        grad_add(g + k, comp ? comp + k : nullptr, v[k]);
+        if (comp && err[k] != 0.0f) atomicAdd(comp + k, err[k]);
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // backward: path replay ("radiative backprop") of referenceBwdOptix.cu:27-74
 
@@ -640,11 +683,8 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const Repla
                 const float w = r.alpha * tr;
                 float* g = B.particle_material_grad + 5 * (size_t)id;
                 float* cg = B.particle_material_comp ? B.particle_material_comp + 5 * (size_t)id : nullptr;
-                grad_add(g + 0, cg ? cg + 0 : nullptr, w * da.x);
-                grad_add(g + 1, cg ? cg + 1 : nullptr, w * da.y);
-                grad_add(g + 2, cg ? cg + 2 : nullptr, w * da.z);
-                grad_add(g + 3, cg ? cg + 3 : nullptr, w * dr);
-                if (metallic_on) grad_add(g + 4, cg ? cg + 4 : nullptr, w * dm);
+                float row[5] = {w * da.x, w * da.y, w * da.z, w * dr, w * dm};
+                grad_add_row(P.flags, g, cg, row, metallic_on ? 5 : 4);
                 tr *= (1.0f - r.alpha);
             }
             start = fmaxf(start, kt[i]);
@@ -666,9 +706,8 @@ PTIR_DEV float3 env_radiance_bwd(const Ctx& C, const BwdInputs& B, float3 d, flo
             const size_t texel = 4 * ((size_t)y * E.w + x);
             float* g = B.environment_grad + texel;
             float* c = B.environment_comp ? B.environment_comp + texel : nullptr;
-            grad_add(g + 0, c ? c + 0 : nullptr, w * cg.x);
-            grad_add(g + 1, c ? c + 1 : nullptr, w * cg.y);
-            grad_add(g + 2, c ? c + 2 : nullptr, w * cg.z);
+            float row[3] = {w * cg.x, w * cg.y, w * cg.z};
+            grad_add_row(C.P.flags, g, c, row, 3);
         };
         add(f.x0, f.y0, f.w00);
         add(f.x1, f.y0, f.w10);

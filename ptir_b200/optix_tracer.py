@@ -85,7 +85,9 @@ class OptixTracer:
     reference). ``storage`` ("fp32",
     "bf16" or "fp16") sets how the tracer holds the Gaussians' attributes: in 16-bit storage
     geometry, material, shading normals and SH are rounded once per call (and by ``build_bvh``)
-    and widened on load, all arithmetic staying FP32."""
+    and widened on load, all arithmetic staying FP32. ``warp_aggregate`` sums the gradient terms
+    that lanes of a warp add to the same Gaussian or texel before the atomics (off: one atomic
+    per lane and term)."""
 
     def __init__(
         self,
@@ -114,6 +116,7 @@ class OptixTracer:
         exact_replay: bool = False,
         compensated_grads: bool = True,
         storage: str = "fp32",
+        warp_aggregate: bool = True,
     ):
         if pipeline not in ("reference",):
             raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
@@ -130,7 +133,7 @@ class OptixTracer:
             int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
             N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
             int(bool(collect_timings)), 0 if sort_rays else 1, int(bool(exact_replay)), 0 if compensated_grads else 1,
-            N.STORAGES[storage])
+            N.STORAGES[storage], 0 if warp_aggregate else 1)
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:

@@ -103,6 +103,43 @@ def test_compensated_gradient_sums(cuda_device):
     assert float(np.quantile(spread, 0.999)) <= 2.5e-7, float(np.quantile(spread, 0.999))
 
 
+@pytest.mark.parametrize("schedule", ["wavefront", "megakernel"])
+def test_warp_aggregated_gradient_sums(cuda_device, schedule):
+    """Warp-aggregated scatter (lanes adding to the same Gaussian or texel sum first, one atomic
+    per row) against one atomic per lane and term: the material and environment gradients agree
+    to float summation order, and they are as close to the FP64 oracle's replay as the per-lane
+    sums. Few large Gaussians and a small environment make rows shared within warps common."""
+    s = small_scene(n=150, w=64, h=64, spp=2, max_bounces=3, scale_range=(0.08, 0.25), env_hw=(8, 16))
+    cfg = O.OracleConfig()
+    ref, _, _ = O.trace(cfg, s, "f64")
+    rng = np.random.default_rng(17)
+    zhw = s["ray_ori"].shape[:3]
+    grads = dict(pbr=rng.standard_normal(zhw + (3,)).astype(np.float32),
+                 light=0.1 * rng.standard_normal(zhw + (3,)).astype(np.float32),
+                 material=rng.standard_normal(zhw + (5,)).astype(np.float32))
+    mg_ref, eg_ref, _ = O.trace_bwd(cfg, s, ref, grads, "f64")
+    S = to_torch(s)
+    res = {}
+    for agg in (True, False):
+        tr = make_tracer(schedule=schedule, warp_aggregate=agg)
+        fwd = list(gpu_trace(tr, S))
+        fwd[10] = torch.from_numpy(ref["pbr"]).cuda()
+        fwd[11] = torch.from_numpy(ref["light"]).cuda()
+        g = {k: torch.from_numpy(v).cuda() for k, v in grads.items()}
+        _, mg, _, _, eg = gpu_trace_bwd(tr, S, fwd, g["pbr"], g["light"], g["material"])
+        torch.cuda.synchronize()
+        assert tr.device_status() == 0
+        res[agg] = (mg.cpu().numpy()[:, :4], eg.cpu().numpy()[..., :3])
+    for k in range(2):
+        rel, _ = _rel_cos(res[True][k], res[False][k])
+        assert rel <= 1e-5, (k, rel)
+    rel_m = {a: _rel_cos(res[a][0], mg_ref[:, :4])[0] for a in res}
+    rel_e = {a: _rel_cos(res[a][1], eg_ref[..., :3])[0] for a in res}
+    # the distance to the oracle is that of the FP32 paths (the same with either scatter)
+    assert rel_m[True] <= rel_m[False] * 1.05 + 1e-7 and rel_e[True] <= rel_e[False] * 1.05 + 1e-7, (rel_m, rel_e)
+    assert rel_m[True] <= 5e-3 and rel_e[True] <= 2e-3, (rel_m, rel_e)
+
+
 def test_backward_sh_indirect_mode(cuda_device):
     """The adjoint in RenderOpts.INDIRECT mode (environment.cuh:733-760) against the oracle."""
     s = small_scene(n=2000, w=40, h=32, spp=2, max_bounces=3, sh_full=True)
