@@ -615,6 +615,13 @@ def accuracy_sample(args, shape: dict, device, name: str = "field-300k-sh", res=
                           z(fwd[3]), z(fwd[4]), z(fwd[5]), z(fwd[6]), z(fwd[7]), torch.from_numpy(g).to(device),
                           z(fwd[11]), 0, 3, 0.001, wl.max_bounces)
         mg, eg = bw[1].cpu().numpy(), bw[4].cpu().numpy()
+        if storage == "fp32":
+            # yardstick: the same estimator in float32 on the CPU (the oracle's FP32 instantiation)
+            r32, _, _ = O.trace(cfg, scene, "f32")
+            e32 = np.abs(r32["pbr"].astype(np.float64) - ref["pbr"].astype(np.float64))
+            out["oracle_fp32_vs_fp64"] = {
+                "pbr_within_1e-3": round(float(np.all(e32 <= 1e-3 + 1e-3 * np.abs(ref["pbr"]), axis=-1).mean()), 5),
+                "pbr_rel_l2": rel_cos(r32["pbr"], ref["pbr"])[0], "pbr_max_abs": float(e32.max())}
         err = np.abs(pbr.astype(np.float64) - ref["pbr"].astype(np.float64))
         ok = np.all(err <= 1e-3 + 1e-3 * np.abs(ref["pbr"]), axis=-1)
         m_rel, m_cos = rel_cos(mg[:, :4], mg_ref[:, :4])
