@@ -304,6 +304,8 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, kbuffer=args.kbuffer)
     if args.no_warp_aggregate:
         shape = dict(shape, warp_aggregate=False)
+    if args.schedule == "megakernel":
+        shape = dict(shape, schedule="megakernel")
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     # target image: the same scene with albedo perturbed by N(0, 0.02)
@@ -654,6 +656,8 @@ def main():
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error report against the FP64 oracle")
+    ap.add_argument("--schedule", default="wavefront", choices=("wavefront", "megakernel"),
+                    help="megakernel: one thread per whole path, the plain drop-in schedule (use with --no-autotune)")
     ap.add_argument("--no-warp-aggregate", action="store_true",
                     help="one gradient atomic per lane and term (default: warp-aggregated rows)")
     ap.add_argument("--kbuffer", type=int, default=0, choices=(0, 8, 16, 24, 32),
