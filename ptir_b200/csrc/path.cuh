@@ -636,59 +636,80 @@ struct ReplayJob {
     unsigned self_occ;
 };
 
-// material gradient of the Gaussians composited along a segment (pathTracer.cuh:313-390)
-template <class Ctx>
-PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const ReplayJob& j) {
-    const bool self_occ = j.self_occ != 0u;
-    const float3 o = j.o, d = j.d;
-    float3 da = j.da;
-    float dr = j.dr, dm = j.dm;
-    const float opacity = j.opacity, max_hit = j.max_hit;
-    const TraceParams& P = C.P;
-    ++C.ctr.replay;
-    const float inv = 1.0f / fmaxf(opacity, 1e-12f);
-    da = da * inv;
-    dr *= inv;
-    dm *= inv;
-    const bool metallic_on = (P.flags & kMetallic) != 0;
-    const float2 clip = clip_scene(P, o, d);
-    float start = fmaxf(0.0f, clip.x - 1e-9f);
+// A replay job in progress: its ray, the per-opacity material gradient it scatters, the
+// interval still to re-traverse and the transmittance so far.
+struct ReplayState {
+    float3 o, d, da;
+    float dr, dm, start, end, tr;
+    bool self_occ;
+};
+
+PTIR_DEV void replay_begin(const TraceParams& P, const ReplayJob& j, ReplayState& r, TraceCounters& ctr) {
+    ++ctr.replay;
+    r.self_occ = j.self_occ != 0u;
+    r.o = j.o;
+    r.d = j.d;
+    const float inv = 1.0f / fmaxf(j.opacity, 1e-12f);
+    r.da = j.da * inv;
+    r.dr = j.dr * inv;
+    r.dm = j.dm * inv;
+    const float2 clip = clip_scene(P, r.o, r.d);
+    r.start = fmaxf(0.0f, clip.x - 1e-9f);
     // The reference ends the re-traversal at max_hit + 1e-9 in float: beyond t ~ 0.017 that is
     // max_hit itself, and with the strict t < tend test the segment's last composited Gaussian
     // gets no gradient. kExactReplay extends the end by one float step to include it.
-    const float end = (P.flags & kExactReplay) ? nextafterf(fminf(max_hit, clip.y), 3.0e38f)
-                                               : fminf(max_hit, clip.y) + 1e-9f;
-    float tr = 1.0f;
+    r.end = (P.flags & kExactReplay) ? nextafterf(fminf(j.max_hit, clip.y), 3.0e38f) : fminf(j.max_hit, clip.y) + 1e-9f;
+    r.tr = 1.0f;
+}
+
+PTIR_DEV bool replay_open(const TraceParams& P, const ReplayState& r) {
+    return r.start < r.end && r.tr > P.min_transmittance;
+}
+
+// Scatter the material gradient onto the accepted hits of one k-buffer batch, front to back.
+template <int K>
+PTIR_DEV void replay_batch(const TraceParams& P, const BwdInputs& B, ReplayState& r, const float (&kt)[K],
+                           const unsigned (&kid)[K], TraceCounters& ctr) {
+    const bool metallic_on = (P.flags & kMetallic) != 0;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        const unsigned id = kid[i];
+        if (id == kNoHit || !(r.tr > P.min_transmittance)) continue;
+        if (r.self_occ && self_occluded(P, kt[i], id, r.d)) {
+            r.start = fmaxf(r.start, kt[i]);
+            continue;
+        }
+        float dns;
+        const Response res = respond(P, id, r.o, r.d, dns);
+        if (res.gres > P.min_response && res.alpha > P.alpha_min) {
+            ++ctr.replay_accepted;
+            const float w = res.alpha * r.tr;
+            float* g = B.particle_material_grad + 5 * (size_t)id;
+            float* cg = B.particle_material_comp ? B.particle_material_comp + 5 * (size_t)id : nullptr;
+            float row[5] = {w * r.da.x, w * r.da.y, w * r.da.z, w * r.dr, w * r.dm};
+            grad_add_row(P.flags, g, cg, row, metallic_on ? 5 : 4);
+            r.tr *= (1.0f - res.alpha);
+        }
+        r.start = fmaxf(r.start, kt[i]);
+    }
+}
+
+// pathTracer.cuh:313-390: one re-traversal that scatters a material gradient onto its Gaussians
+template <class Ctx>
+PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const ReplayJob& j) {
+    const TraceParams& P = C.P;
+    ReplayState r;
+    replay_begin(P, j, r, C.ctr);
     float kt[Ctx::K];
     unsigned kid[Ctx::K];
-    for (int round = 0; start < end && tr > P.min_transmittance; ++round) {
+    for (int round = 0; replay_open(P, r); ++round) {
         if (round > (1 << 16)) {
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
-        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
+        trace_kbuf(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
-#pragma unroll
-        for (int i = 0; i < Ctx::K; ++i) {
-            const unsigned id = kid[i];
-            if (id == kNoHit || !(tr > P.min_transmittance)) continue;
-            if (self_occ && self_occluded(P, kt[i], id, d)) {
-                start = fmaxf(start, kt[i]);
-                continue;
-            }
-            float dns;
-            const Response r = respond(P, id, o, d, dns);
-            if (r.gres > P.min_response && r.alpha > P.alpha_min) {
-                ++C.ctr.replay_accepted;
-                const float w = r.alpha * tr;
-                float* g = B.particle_material_grad + 5 * (size_t)id;
-                float* cg = B.particle_material_comp ? B.particle_material_comp + 5 * (size_t)id : nullptr;
-                float row[5] = {w * da.x, w * da.y, w * da.z, w * dr, w * dm};
-                grad_add_row(P.flags, g, cg, row, metallic_on ? 5 : 4);
-                tr *= (1.0f - r.alpha);
-            }
-            start = fmaxf(start, kt[i]);
-        }
+        replay_batch(P, B, r, kt, kid, C.ctr);
     }
 }
 
