@@ -39,6 +39,7 @@ struct WfView {
     unsigned* count;         // [kNumQueueCounts]
     unsigned* cursor;        // [kNumCursors]
     ReplayJob* jobs;
+    float* parked;           // intersection: parked accumulators and k-buffer batches, per thread
     unsigned long long tile0;  // first tile of the chunk
     unsigned slots;          // paths in the chunk (32 per tile)
 };
@@ -152,9 +153,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_sort_keys(TraceParams P, WfV
 
 PTIR_DEV unsigned lanes_below() { return (1u << lane()) - 1u; }
 
-// The compositing accumulators of a lane's segment, parked in shared memory while its warp
-// traverses (they are only touched between trace calls), so that they hold no registers during
-// the traversal: one float per field and thread, field-major (no bank conflicts).
+// The compositing accumulators of a lane's segment, parked in global memory while its warp
+// traverses (they are only touched between trace calls, about three times per segment, and stay
+// in L2), so that they hold no registers during the traversal and no shared memory: L1 keeps
+// all of its capacity for node and leaf records. One float per field and thread, field-major
+// with the grid's thread count as stride (coalesced).
 constexpr int kParkedFields = 22;
 
 struct Parked {
@@ -189,8 +192,8 @@ struct Parked {
 // and starts the next call, or writes its segment, hands it to queue `out_q` (when >= 0) and
 // takes the next one from the queue, so that no lane waits for the slowest segment of its warp.
 // The warp leaves its traversal loop once `refill` lanes wait (a finished call, or idle while
-// the queue still holds segments). Launched with parked_bytes(block, K) of shared memory: the
-// parked accumulators and, while a batch is composited, its k-buffer.
+// the queue still holds segments). W.parked holds, per thread of the grid, the parked
+// accumulators and, while a batch is composited, its k-buffer (kParkedFields + 2K floats).
 // Registers per thread of k_wf_trace: 96 lets five 128-thread blocks share an SM (four at the
 // compiler's own choice of 128), which measured 5 % faster on the 1M-Gaussian scene despite a few
 // spills; the 32-entry k-buffer variant gets 168 (three blocks: keeping its ids in shared memory
@@ -200,10 +203,11 @@ constexpr int trace_regs(int K) { return K > 16 ? 168 : 96; }
 template <int K, bool kMark, bool kSelfOcc>
 __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
                                                       const unsigned* items, int out_q, unsigned cursor, int refill) {
-    extern __shared__ float wf_parked[];
-    const Parked pk{wf_parked + threadIdx.x, (int)blockDim.x};
-    float* const batch_t = wf_parked + kParkedFields * blockDim.x + threadIdx.x;
-    unsigned* const batch_id = reinterpret_cast<unsigned*>(batch_t + K * blockDim.x);
+    const int nthreads = (int)(gridDim.x * blockDim.x);
+    float* const base = W.parked + blockIdx.x * blockDim.x + threadIdx.x;
+    const Parked pk{base, nthreads};
+    float* const batch_t = base + kParkedFields * nthreads;
+    unsigned* const batch_id = reinterpret_cast<unsigned*>(batch_t + K * nthreads);
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -280,11 +284,10 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
                 // the batch goes to shared memory, so compositing holds no k-buffer registers
 #pragma unroll
                 for (int i = 0; i < K; ++i) {
-                    batch_t[i * blockDim.x] = kt[i];
-                    batch_id[i * blockDim.x] = kid[i];
+                    batch_t[i * nthreads] = kt[i];
+                    batch_id[i * nthreads] = kid[i];
                 }
-                composite_hits_strided<kSelfOcc, K>(P, ctr, c, batch_t, batch_id, (int)blockDim.x,
-                                                    kMark ? vis : nullptr);
+                composite_hits_strided<kSelfOcc, K>(P, ctr, c, batch_t, batch_id, nthreads, kMark ? vis : nullptr);
                 next_call(c);
             }
             // nothing found, segment closed, or loop bound: the segment is complete
@@ -664,8 +667,16 @@ int grid_for(const void* fn, int block, size_t smem) {
     return sms * per_sm;
 }
 
-// dynamic shared memory of k_wf_trace<K> at a block size
-size_t parked_bytes(int block, int K) { return sizeof(float) * (kParkedFields + 2 * K) * (size_t)block; }
+// floats of W.parked for every thread the device can hold resident (k-buffer up to 32)
+size_t parked_floats() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev);
+    if (sms <= 0) sms = 148;
+    if (per_sm <= 0) per_sm = 2048;
+    return (size_t)(kParkedFields + 2 * 32) * (size_t)sms * (size_t)per_sm;
+}
 
 // grid of a kernel at a block size, computed once per (kernel, block size)
 int grid_cached(const void* fn, int block, size_t smem = 0) {
@@ -690,7 +701,7 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
         if (p) cudaFreeAsync(p, s);
     };
     rel(b.seg); rel(b.ps); rel(b.rng); rel(b.q[0]); rel(b.q[1]); rel(b.q[2]); rel(b.jobs);
-    rel(b.sort_keys[0]); rel(b.sort_keys[1]); rel(b.sorted); rel(b.sort_temp);
+    rel(b.sort_keys[0]); rel(b.sort_keys[1]); rel(b.sorted); rel(b.sort_temp); rel(b.parked);
     void* counters = b.counters;
     b = WavefrontBuffers{};
     b.counters = counters;
@@ -707,6 +718,7 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
     get(&b.sort_keys[0], sizeof(unsigned) * slots);
     get(&b.sort_keys[1], sizeof(unsigned) * slots);
     get(&b.sorted, sizeof(unsigned) * slots);
+    get(&b.parked, sizeof(float) * parked_floats());
     if (e == cudaSuccess) {
         size_t bytes = 0;
         e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
@@ -720,7 +732,7 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
 
 void wavefront_free(WavefrontBuffers& b) {
     for (void* p : {b.seg, b.ps, b.rng, b.q[0], b.q[1], b.q[2], b.jobs, b.counters, b.sort_keys[0], b.sort_keys[1],
-                    b.sorted, b.sort_temp})
+                    b.sorted, b.sort_temp, b.parked})
         if (p) cudaFree(p);
     b = WavefrontBuffers{};
 }
@@ -734,6 +746,7 @@ static WfView view_of(const WavefrontBuffers& b, unsigned long long tile0, unsig
     W.count = static_cast<unsigned*>(b.counters);
     W.cursor = W.count + kNumQueueCounts;
     W.jobs = static_cast<ReplayJob*>(b.jobs);
+    W.parked = static_cast<float*>(b.parked);
     W.tile0 = tile0;
     W.slots = slots;
     return W;
@@ -776,8 +789,8 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
     const int g_primary = grid_cached((const void*)k_wf_fwd_primary<K>, B);
     const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
     const int g_bounce = grid_cached((const void*)k_wf_fwd_bounce<K>, B);
-    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B, parked_bytes(B, K));
-    const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B, parked_bytes(B, K));
+    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B);
+    const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B);
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 2u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
@@ -790,7 +803,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            k_wf_trace<K, true, false><<<std::min(g_trace0, cap), B, parked_bytes(B, K), s>>>(q, o.visibility, W, kQIsect,
+            k_wf_trace<K, true, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, o.visibility, W, kQIsect,
                                                                              W.q[kQIsect], -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
@@ -809,7 +822,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                k_wf_trace<K, true, true><<<g_trace, B, parked_bytes(B, K), s>>>(q, o.visibility, W, kQIsect, items, kQBounce, cursor,
+                k_wf_trace<K, true, true><<<g_trace, B, 0, s>>>(q, o.visibility, W, kQIsect, items, kQBounce, cursor,
                                                                 R);
             });
             ++cursor;
@@ -833,8 +846,8 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
     const int g_primary = grid_cached((const void*)k_wb_primary<K>, B);
     const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
     const int g_bounce = grid_cached((const void*)k_wb_bounce<K>, B);
-    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B, parked_bytes(B, K));
-    const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B, parked_bytes(B, K));
+    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B);
+    const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B);
     const int g_replay = grid_cached((const void*)k_wb_replay<K>, B);
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
@@ -848,7 +861,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            k_wf_trace<K, false, false><<<std::min(g_trace0, cap), B, parked_bytes(B, K), s>>>(q, nullptr, W, kQIsect, W.q[kQIsect],
+            k_wf_trace<K, false, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, nullptr, W, kQIsect, W.q[kQIsect],
                                                                               -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
@@ -872,7 +885,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                k_wf_trace<K, false, true><<<g_trace, B, parked_bytes(B, K), s>>>(q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
+                k_wf_trace<K, false, true><<<g_trace, B, 0, s>>>(q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
             });
             ++cursor;
         }

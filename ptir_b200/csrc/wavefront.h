@@ -25,6 +25,7 @@ struct WavefrontBuffers {
     void* sorted = nullptr;  // u32[slots]: the intersect queue in key order
     void* sort_temp = nullptr;
     size_t sort_temp_bytes = 0;
+    void* parked = nullptr;  // f32, per resident thread of the intersection kernel (k_wf_trace)
 };
 
 cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s);
