@@ -88,6 +88,8 @@ typedef struct ptir_config {
     int32_t grad_aggregate;       /* gradient scatter: 0 = lanes of a warp that add to the same Gaussian or
                                      texel sum their terms first and one of them issues the atomics
                                      (default), 1 = one atomic per lane and term as the reference */
+    int32_t shadow_kbuffer;       /* wavefront: candidates per NEE shadow-ray traversal, 8, 16 or 32 (0 = 16);
+                                     a shadow walk visits hits in distance order whatever the size */
 } ptir_config;
 
 enum { PTIR_STORAGE_FP32 = 0, PTIR_STORAGE_BF16 = 1, PTIR_STORAGE_FP16 = 2 };

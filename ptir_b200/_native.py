@@ -43,6 +43,7 @@ class PtirConfig(C.Structure):
         ("grad_sums", C.c_int32),
         ("storage", C.c_int32),
         ("grad_aggregate", C.c_int32),
+        ("shadow_kbuffer", C.c_int32),
     ]
 
 

@@ -57,6 +57,7 @@ ptir::WavefrontTuning tuning_of(const ptir_config& c) {
     ptir::WavefrontTuning w;
     if (c.chunk_tiles > 0) w.chunk_tiles = (unsigned)c.chunk_tiles;
     if (c.kbuffer > 0) w.kbuf = c.kbuffer;
+    if (c.shadow_kbuffer > 0) w.shadow_kbuf = c.shadow_kbuffer;
     if (c.refill_lanes > 0) w.refill_lanes = c.refill_lanes;
     if (c.block_size > 0) w.block = c.block_size;
     w.sort_rays = c.ray_order == 0;
@@ -274,6 +275,9 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     if (config->schedule != PTIR_SCHEDULE_WAVEFRONT && config->schedule != PTIR_SCHEDULE_MEGAKERNEL) return PTIR_EINVAL;
     if (config->chunk_tiles < 0) return PTIR_EINVAL;
     if (!(config->kbuffer == 0 || config->kbuffer == 8 || config->kbuffer == 16 || config->kbuffer == 32)) return PTIR_EINVAL;
+    if (!(config->shadow_kbuffer == 0 || config->shadow_kbuffer == 8 || config->shadow_kbuffer == 16 ||
+          config->shadow_kbuffer == 32))
+        return PTIR_EINVAL;
     if (config->refill_lanes < 0 || config->refill_lanes > 32) return PTIR_EINVAL;
     if (!(config->block_size == 0 || config->block_size == 64 || config->block_size == 128 || config->block_size == 256))
         return PTIR_EINVAL;

@@ -652,6 +652,20 @@ __global__ void __launch_bounds__(kMaxThreads) k_wb_replay(TraceParams P, BwdInp
     flush_counters(P, ctr);
 }
 
+// persistent grid: resident blocks per SM x SMs (defined below)
+int grid_cached(const void* fn, int block, size_t smem);
+
+// The shadow stage with its own k-buffer size. A shadow walk visits the hits in distance order
+// until one occludes, whatever the batch size, so its size is free of the intersection's: a
+// walk usually ends in its first batch, which a smaller buffer gathers with less traversal.
+static void launch_shadow(int ks, const TraceParams& q, const WfView& W, int B, int R, cudaStream_t s) {
+    switch (ks) {
+    case 8: k_wf_shadow<8><<<grid_cached((const void*)k_wf_shadow<8>, B, 0), B, 0, s>>>(q, W, R); break;
+    case 32: k_wf_shadow<32><<<grid_cached((const void*)k_wf_shadow<32>, B, 0), B, 0, s>>>(q, W, R); break;
+    default: k_wf_shadow<16><<<grid_cached((const void*)k_wf_shadow<16>, B, 0), B, 0, s>>>(q, W, R); break;
+    }
+}
+
 // persistent grid: resident blocks per SM x SMs
 int grid_for(const void* fn, int block, size_t smem) {
     static int sms = 0;
@@ -787,7 +801,6 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
     const int B = tune.block, R = tune.refill_lanes;
     const int g_camera = grid_cached((const void*)k_wf_camera, B);
     const int g_primary = grid_cached((const void*)k_wf_fwd_primary<K>, B);
-    const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
     const int g_bounce = grid_cached((const void*)k_wf_fwd_bounce<K>, B);
     const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B);
     const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B);
@@ -810,7 +823,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             k_wf_fwd_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, o, W);
         });
         if (p.flags & kMis)
-            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { k_wf_shadow<K><<<g_shadow, B, 0, s>>>(q, W, R); });
+            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { launch_shadow(tune.shadow_kbuf, q, W, B, R, s); });
         unsigned cursor = kFirstBounceCursor;
         for (unsigned depth = 0; depth < mb; ++depth) {
             cudaMemsetAsync(W.count + kQIsect, 0, sizeof(unsigned), s);
@@ -844,7 +857,6 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
     const int B = tune.block, R = tune.refill_lanes;
     const int g_camera = grid_cached((const void*)k_wf_camera, B);
     const int g_primary = grid_cached((const void*)k_wb_primary<K>, B);
-    const int g_shadow = grid_cached((const void*)k_wf_shadow<K>, B);
     const int g_bounce = grid_cached((const void*)k_wb_bounce<K>, B);
     const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B);
     const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B);
@@ -868,7 +880,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             k_wb_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, bi, W);
         });
         if (p.flags & kMis)
-            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { k_wf_shadow<K><<<g_shadow, B, 0, s>>>(q, W, R); });
+            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { launch_shadow(tune.shadow_kbuf, q, W, B, R, s); });
         unsigned cursor = kFirstBounceCursor;
         for (unsigned depth = 0; depth < mb; ++depth) {
             cudaMemsetAsync(W.count + kQIsect, 0, sizeof(unsigned), s);

@@ -39,6 +39,7 @@ struct WavefrontTuning {
     int refill_lanes = 32;          // intersection: waiting lanes (1..32) before a warp refills
     int block = 128;                // threads per block: 64, 128 or 256
     bool sort_rays = true;          // intersect bounce rays in (direction octant, origin cell) order
+    int shadow_kbuf = 16;           // candidates per shadow-ray traversal: 8, 16 or 32
 };
 
 cudaError_t launch_trace_fwd_wavefront(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b,
