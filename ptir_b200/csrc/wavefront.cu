@@ -194,11 +194,12 @@ struct Parked {
 // The warp leaves its traversal loop once `refill` lanes wait (a finished call, or idle while
 // the queue still holds segments). W.parked holds, per thread of the grid, the parked
 // accumulators and, while a batch is composited, its k-buffer (kParkedFields + 2K floats).
-// Registers per thread of k_wf_trace: 96 lets five 128-thread blocks share an SM (four at the
-// compiler's own choice of 128), which measured 5 % faster on the 1M-Gaussian scene despite a few
-// spills; the 32-entry k-buffer variant gets 168 (three blocks: keeping its ids in shared memory
-// instead, for four blocks, measured slower).
-constexpr int trace_regs(int K) { return K > 16 ? 168 : 96; }
+// Registers per thread of k_wf_trace (and of the shadow kernel of the same k-buffer size). The
+// kernels use no shared memory, so registers alone set the resident warps. K <= 16: 96, five
+// 128-thread blocks per SM, 5 % faster than the compiler's own 127 (four blocks) despite a few
+// spills; 80 (six blocks) was 11 % slower. K = 32: 128, four blocks, 6 % faster for the step
+// than 168 (three blocks); 96 (five blocks) was 23 % slower.
+constexpr int trace_regs(int K) { return K > 16 ? 128 : 96; }
 
 template <int K, bool kMark, bool kSelfOcc>
 __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
