@@ -162,7 +162,7 @@ constexpr int kParkedFields = 22;
 
 struct Parked {
     float* base;  // this thread's first field
-    int stride;   // threads per block
+    int stride;   // threads of the grid
     __device__ __forceinline__ float& f(int k) const { return base[k * stride]; }
     __device__ __forceinline__ void save(const Composite& c) const {
         f(0) = c.radiance.x; f(1) = c.radiance.y; f(2) = c.radiance.z;
