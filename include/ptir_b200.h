@@ -65,8 +65,10 @@ typedef struct ptir_config {
     /* B200 schedule (render.b200.*; no counterpart in the reference, results are identical): */
     int32_t schedule;             /* PTIR_SCHEDULE_WAVEFRONT (default) or PTIR_SCHEDULE_MEGAKERNEL */
     int32_t chunk_tiles;          /* wavefront: 8x4 pixel tiles per chunk of paths (0 = default 131072) */
-    int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16). The
-                                     hits are composited in the same order for every size. */
+    int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16, the
+                                     reference's). Another size culls subtrees at another distance and
+                                     keeps another set of grazing candidates (closest approach before
+                                     their box entry), which changes a small share of the samples. */
     int32_t refill_lanes;         /* wavefront intersection: waiting lanes, 1..32, before a warp refills (0 = 32) */
     int32_t block_size;           /* wavefront: threads per block, 64, 128 or 256 (0 = 128) */
     int32_t collect_timings;      /* record CUDA events around every kernel launch (ptir_get_stage_times) */

@@ -11,8 +11,9 @@
 // against [tmin, t_K], where t_K is the K-th distance found so far (the reference's any-hit
 // program shrinks the ray's tmax to the 16th distance). This returns the K nearest candidates
 // except for a Gaussian whose closest approach lies before its own box entry (a ray grazing a
-// box corner, where the kernel response is below the acceptance threshold): like the
-// reference, it is then kept only if reached before t_K drops below its box entry.
+// box corner): like the reference, it is then kept only if reached before t_K drops below its
+// box entry. Its response can pass the acceptance threshold, so K (which sets t_K) can change
+// the image; K = 16 is the reference's.
 #pragma once
 
 #include "device_types.h"

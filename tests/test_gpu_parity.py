@@ -127,8 +127,8 @@ def test_wavefront_and_megakernel_agree(cuda_device, chunk_tiles, kbuffer):
         close = torch.isclose(a2, b2, rtol=1e-5, atol=1e-6).all(dim=-1).float().mean().item()
         assert close >= 0.995, (k, close)
     # A k-buffer size other than the reference's 16 culls subtrees at a different distance. It can
-    # then keep a different rejected grazing candidate, which moves a segment's last-hit distance,
-    # the end of its backward re-traversal. Other sizes get 1 %.
+    # then keep a different set of grazing candidates, which changes a few samples and moves
+    # segments' last-hit distances, the ends of the backward re-traversals. Other sizes get 1 %.
     tol = 2e-3 if kbuffer == 16 else 1e-2
     for a, b in zip(grads["megakernel"], grads["wavefront"]):
         a, b = a.double().reshape(-1), b.double().reshape(-1)
