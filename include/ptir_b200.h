@@ -72,7 +72,7 @@ typedef struct ptir_config {
     int32_t refill_lanes;         /* wavefront intersection: waiting lanes, 1..32, before a warp refills (0 = 32) */
     int32_t block_size;           /* wavefront: threads per block, 64, 128 or 256 (0 = 128) */
     int32_t collect_timings;      /* record CUDA events around every kernel launch (ptir_get_stage_times) */
-    int32_t ray_order;            /* wavefront bounce rays: 0 = intersected in (direction octant, origin cell)
+    int32_t ray_order;            /* wavefront bounce rays: 0 = intersected in (octant, origin cell, direction cell)
                                      order (default), 1 = in queue order; results are the same */
     int32_t exact_replay;         /* 0 = the reference's adjoint: backward re-traversals end where its float
                                      epsilon leaves out each segment's last composited Gaussian, and the

@@ -38,7 +38,7 @@ struct WavefrontTuning {
     int kbuf = 16;                  // candidates per traversal: 8, 16 or 32
     int refill_lanes = 32;          // intersection: waiting lanes (1..32) before a warp refills
     int block = 128;                // threads per block: 64, 128 or 256
-    bool sort_rays = true;          // intersect bounce rays in (direction octant, origin cell) order
+    bool sort_rays = true;          // intersect bounce rays in (octant, origin cell, direction cell) order
     int shadow_kbuf = 16;           // candidates per shadow-ray traversal: 8, 16 or 32
 };
 

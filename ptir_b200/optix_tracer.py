@@ -78,7 +78,7 @@ class OptixTracer:
     traversal), ``refill_lanes`` (waiting lanes before an intersection warp refills, 1..32) and
     ``block_size`` (64, 128 or 256); 0 keeps the default. ``collect_timings`` records CUDA events
     around every kernel launch for ``stage_times()``; ``sort_rays`` intersects bounce rays in
-    (direction octant, origin cell) order (the results do not change); ``exact_replay`` lets the
+    (direction octant, origin cell, direction cell) order (the results do not change); ``exact_replay`` lets the
     backward re-traversals include each segment's last composited Gaussian, which the
     reference's float epsilon leaves out; ``compensated_grads``
     accumulates the gradient atomics as Kahan pairs (off: plain float atomics, as the
