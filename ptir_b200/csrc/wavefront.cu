@@ -127,6 +127,8 @@ PTIR_DEV unsigned spread3_8(unsigned v) {
     return v;
 }
 
+// Keys of queue in_q: the intersect queue's segment rays, or the shadow queue's rays toward their
+// light samples.
 __global__ void __launch_bounds__(kMaxThreads) k_wf_sort_keys(TraceParams P, WfView W, int in_q, unsigned* keys) {
     const unsigned count = W.count[in_q];
     float3 lo = f3(0.0f), scale = f3(0.0f);
@@ -140,7 +142,11 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_sort_keys(TraceParams P, WfV
         unsigned key = kSortPad;
         if (i < count) {
             const unsigned q = W.q[in_q][i];
-            const float3 o = W.seg[q].o, d = W.seg[q].d;
+            float3 o = W.seg[q].o, d = W.seg[q].d;
+            if (in_q == kQShadow) {
+                d = W.ps[q].em.dir;
+                o = W.seg[q].pos + d * 2e-2f;
+            }
             const unsigned oct = (d.x < 0.0f ? 4u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 1u : 0u);
             const float3 c = (o - lo) * scale * (1.0f / 16.0f);
             const unsigned cx = (unsigned)fminf(fmaxf(c.x, 0.0f), 15.0f);
@@ -404,7 +410,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_primary(TraceParams P, F
 // walk this cut the stage by 15 % on the 1M-Gaussian scene, and the register cap of the
 // intersection kernel (more resident warps) by 6 % more.
 template <int K>
-__global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, int refill) {
+__global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, int refill, const unsigned* items) {
     int stack[kStackDepth];
     float stack_t[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -443,7 +449,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, 
             if (phase == kIdle) {
                 const unsigned i = base + __popc(idle & lanes_below());
                 if (i < count) {
-                    q = W.q[kQShadow][i];
+                    q = items[i];
                     const float3 wi = W.ps[q].em.dir;
                     ro = W.seg[q].pos + wi * 2e-2f;
                     rd = wi;
@@ -669,11 +675,12 @@ int grid_cached(const void* fn, int block, size_t smem);
 // The shadow stage with its own k-buffer size. A shadow walk visits the hits in distance order
 // until one occludes, whatever the batch size, so its size is free of the intersection's: a
 // walk usually ends in its first batch, which a smaller buffer gathers with less traversal.
-static void launch_shadow(int ks, const TraceParams& q, const WfView& W, int B, int R, cudaStream_t s) {
+static void launch_shadow(int ks, const TraceParams& q, const WfView& W, int B, int R, const unsigned* items,
+                          cudaStream_t s) {
     switch (ks) {
-    case 8: k_wf_shadow<8><<<grid_cached((const void*)k_wf_shadow<8>, B, 0), B, 0, s>>>(q, W, R); break;
-    case 32: k_wf_shadow<32><<<grid_cached((const void*)k_wf_shadow<32>, B, 0), B, 0, s>>>(q, W, R); break;
-    default: k_wf_shadow<16><<<grid_cached((const void*)k_wf_shadow<16>, B, 0), B, 0, s>>>(q, W, R); break;
+    case 8: k_wf_shadow<8><<<grid_cached((const void*)k_wf_shadow<8>, B, 0), B, 0, s>>>(q, W, R, items); break;
+    case 32: k_wf_shadow<32><<<grid_cached((const void*)k_wf_shadow<32>, B, 0), B, 0, s>>>(q, W, R, items); break;
+    default: k_wf_shadow<16><<<grid_cached((const void*)k_wf_shadow<16>, B, 0), B, 0, s>>>(q, W, R, items); break;
     }
 }
 
@@ -782,16 +789,16 @@ static unsigned long long total_tiles(const TraceParams& p) { return (unsigned l
 // The intersect queue in ray order (or as queued when sorting is off): keys, then a key/slot
 // radix sort of the whole chunk capacity (the count stays on the device).
 static const unsigned* sort_queue(const TraceParams& p, const WavefrontBuffers& b, const WfView& W,
-                                  const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s) {
-    if (!tune.sort_rays) return W.q[kQIsect];
+                                  const WavefrontTuning& tune, const StageCtx& sc, cudaStream_t s, int in_q = kQIsect) {
+    if (!tune.sort_rays) return W.q[in_q];
     unsigned* keys_in = static_cast<unsigned*>(b.sort_keys[0]);
     unsigned* keys_out = static_cast<unsigned*>(b.sort_keys[1]);
     unsigned* sorted = static_cast<unsigned*>(b.sorted);
     const int grid = grid_cached((const void*)k_wf_sort_keys, tune.block);
     sc.run(kStageSort, p, s, [&](const TraceParams& q) {
-        k_wf_sort_keys<<<grid, tune.block, 0, s>>>(q, W, kQIsect, keys_in);
+        k_wf_sort_keys<<<grid, tune.block, 0, s>>>(q, W, in_q, keys_in);
         size_t bytes = b.sort_temp_bytes;
-        cub::DeviceRadixSort::SortPairs(b.sort_temp, bytes, keys_in, keys_out, W.q[kQIsect], sorted, (int)W.slots, 0,
+        cub::DeviceRadixSort::SortPairs(b.sort_temp, bytes, keys_in, keys_out, W.q[in_q], sorted, (int)W.slots, 0,
                                         kSortKeyBits, s);
     });
     return sorted;
@@ -833,8 +840,11 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
             k_wf_fwd_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, o, W);
         });
-        if (p.flags & kMis)
-            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { launch_shadow(tune.shadow_kbuf, q, W, B, R, s); });
+        if (p.flags & kMis) {
+            const unsigned* shadow_items = sort_queue(p, b, W, tune, sc, s, kQShadow);
+            sc.run(kStageShadow, p, s,
+                   [&](const TraceParams& q) { launch_shadow(tune.shadow_kbuf, q, W, B, R, shadow_items, s); });
+        }
         unsigned cursor = kFirstBounceCursor;
         for (unsigned depth = 0; depth < mb; ++depth) {
             cudaMemsetAsync(W.count + kQIsect, 0, sizeof(unsigned), s);
@@ -890,8 +900,11 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
             k_wb_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, bi, W);
         });
-        if (p.flags & kMis)
-            sc.run(kStageShadow, p, s, [&](const TraceParams& q) { launch_shadow(tune.shadow_kbuf, q, W, B, R, s); });
+        if (p.flags & kMis) {
+            const unsigned* shadow_items = sort_queue(p, b, W, tune, sc, s, kQShadow);
+            sc.run(kStageShadow, p, s,
+                   [&](const TraceParams& q) { launch_shadow(tune.shadow_kbuf, q, W, B, R, shadow_items, s); });
+        }
         unsigned cursor = kFirstBounceCursor;
         for (unsigned depth = 0; depth < mb; ++depth) {
             cudaMemsetAsync(W.count + kQIsect, 0, sizeof(unsigned), s);
