@@ -281,7 +281,7 @@ def tune_launch_shape(S, args, device) -> dict:
             tr.trace_bwd(0, S.t2w, ori, drs, *args_b)
 
     shapes = autotune.space() if args.autotune_full else autotune.space(kbuffers=(16,), blocks=(64, 128),
-                                                                          chunks=(131072,), refills=(16, 32))
+                                                                          chunks=(0,), refills=(16, 32))
     sig = (f"{S.wl.name}|n={S.wl.n}|samples={S.samples}|bounces={S.wl.max_bounces}|storage={args.storage}"
            f"|shapes={len(shapes)}")
     tuner = autotune.Autotuner(os.path.join(ROOT, "_autotune.json"))
@@ -308,6 +308,8 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, warp_aggregate=False)
     if args.schedule == "megakernel":
         shape = dict(shape, schedule="megakernel")
+    if args.chunk_tiles:
+        shape = dict(shape, chunk_tiles=args.chunk_tiles)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     # target image: the same scene with albedo perturbed by N(0, 0.02)
@@ -658,6 +660,7 @@ def main():
                     help="attribute storage of the tracer (arithmetic is FP32 in every case)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the error report against the FP64 oracle")
+    ap.add_argument("--chunk-tiles", type=int, default=0, help="8x4 pixel tiles per wavefront chunk (0: tuned / default)")
     ap.add_argument("--schedule", default="wavefront", choices=("wavefront", "megakernel"),
                     help="megakernel: one thread per whole path, the plain drop-in schedule (use with --no-autotune)")
     ap.add_argument("--no-warp-aggregate", action="store_true",

@@ -64,7 +64,8 @@ typedef struct ptir_config {
     int32_t collect_counters;     /* keep per-launch segment/candidate counters (cheap) */
     /* B200 schedule (render.b200.*; no counterpart in the reference, results are identical): */
     int32_t schedule;             /* PTIR_SCHEDULE_WAVEFRONT (default) or PTIR_SCHEDULE_MEGAKERNEL */
-    int32_t chunk_tiles;          /* wavefront: 8x4 pixel tiles per chunk of paths (0 = default 131072) */
+    int32_t chunk_tiles;          /* wavefront: 8x4 pixel tiles per chunk of paths (0 = sized at the tracer's
+                                     first trace to a third of the free device memory, at least 32768) */
     int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16, the
                                      reference's). Another size culls subtrees at another distance and
                                      keeps another set of grazing candidates (closest approach before

@@ -23,7 +23,7 @@ import torch
 
 KBUFFERS = (8, 16, 32)
 BLOCKS = (64, 128, 256)
-CHUNKS = (32768, 131072)
+CHUNKS = (0, 131072)  # 0: the tracer sizes its chunk from the free device memory
 REFILLS = (16, 32)
 
 
@@ -31,7 +31,7 @@ REFILLS = (16, 32)
 class Shape:
     kbuffer: int = 16
     block_size: int = 128
-    chunk_tiles: int = 131072
+    chunk_tiles: int = 0
     refill_lanes: int = 32
 
     def launch(self) -> dict:

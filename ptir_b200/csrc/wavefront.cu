@@ -762,6 +762,13 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
     return e;
 }
 
+size_t wavefront_bytes_per_slot() {
+    // path state, RNG, three queues, two replay jobs, two sort keys + the sorted queue, and CUB's
+    // double-buffered radix-sort temporary (about two key / value pairs)
+    return sizeof(Segment) + sizeof(PathState) + sizeof(unsigned long long) + 3 * sizeof(unsigned) +
+           2 * sizeof(ReplayJob) + 3 * sizeof(unsigned) + 4 * sizeof(unsigned);
+}
+
 void wavefront_free(WavefrontBuffers& b) {
     for (void* p : {b.seg, b.ps, b.rng, b.q[0], b.q[1], b.q[2], b.jobs, b.counters, b.sort_keys[0], b.sort_keys[1],
                     b.sorted, b.sort_temp, b.parked})

@@ -29,6 +29,8 @@ struct WavefrontBuffers {
 };
 
 cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s);
+// device bytes the wavefront holds per path slot of a chunk (state, queues, replay jobs, sort)
+size_t wavefront_bytes_per_slot();
 void wavefront_free(WavefrontBuffers& b);
 
 // Launch shape of the wavefront schedule. Only the k-buffer size can change a result: it moves
