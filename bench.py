@@ -1,12 +1,13 @@
 """Benchmark of the Gaussian-field path tracer: forward + adjoint path segments per second.
 
 A step is one inverse-rendering training iteration on the workload: LBVH refit, forward trace of
-every (view, sample) path, L1 loss gradient against a target render, the path-replay adjoint,
-and the fused selective Adam step of the material and environment. The default workload is
-field-1m (1M Gaussians, 8 views of 1024x768 at 16 spp, 4 bounces, 512x1024 environment; see
-ptir_b200/synthetic.py) with BF16 attribute storage and FP32 arithmetic; --storage fp32 gives
-the plain FP32 drop-in. The metric counts the forward path segments of a step (the adjoint
-replays each of them) over the step's device time.
+every (view, sample) path, the loss (the terms of PTIR's default training loss that the tracer's
+outputs feed: L1 on pbr against a target render, L2 albedo and roughness prior regularisation on
+the material output), the path-replay adjoint, and the fused selective Adam step of the material
+and environment. The default workload is field-1m (1M Gaussians, 8 views of 1024x768 at 16 spp,
+4 bounces, 512x1024 environment; see ptir_b200/synthetic.py) with BF16 attribute storage and FP32
+arithmetic; --storage fp32 gives the plain FP32 drop-in. The metric counts the forward path
+segments of a step (the adjoint replays each of them) over the step's device time.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME] [--storage bf16|fp16|fp32]
                   [--impl ours|reference]
@@ -16,8 +17,8 @@ traces its own views of the same scene (weak scaling) and the material / environ
 gradients are summed with one NCCL all-reduce per step.
 
 --impl reference times the reference path's CPU restatement (the oracle port in FP32, all
-host threads) on a bounded sample of the same workload, the reference's OptiX build being
-unavailable here (no OptiX SDK headers).
+host threads) on a bounded sample of the same workload with the same loss, the reference's
+OptiX build being unavailable here (no OptiX SDK headers).
 """
 from __future__ import annotations
 
@@ -42,6 +43,13 @@ from ptir_b200 import envmap, synthetic  # noqa: E402
 from ptir_b200.optim import selective_adam_  # noqa: E402
 
 METRIC = "fwd+bwd path segments/s at 1M Gaussians"
+
+
+def metric_of(wl) -> str:
+    """The metric's name: the headline's for the 1M-Gaussian workload, else named for the workload."""
+    if wl.name == "field-1m":
+        return METRIC
+    return f"{'fwd+bwd' if wl.backward else 'fwd'} path segments/s ({wl.name}, {wl.n:,} Gaussians)"
 ADAM_LR = 1e-3
 PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
 HBM_FALLBACK_GBS = 6650.0
@@ -125,24 +133,27 @@ class Setup:
         return OptixTracer("", "", "reference", "referenceBwd", "instances", 4, 0.0113, True, 3, True, True, True,
                            False, False, **kw)
 
-    def trace(self, tr, material=None, ray_ori=None, ray_dir=None, frame=0):
+    def trace(self, tr, material=None, ray_ori=None, ray_dir=None, frame=0, env=None):
         ori = self.ray_ori if ray_ori is None else ray_ori
         drs = self.ray_dir if ray_dir is None else ray_dir
         mat = self.material if material is None else material
-        scene = (self.density, mat, self.sph, self.snrm, self.env, self.alias, *self.lights, 0, 3, 0.001,
-                 self.wl.max_bounces)
+        scene = (self.density, mat, self.sph, self.snrm, self.env if env is None else env, self.alias, *self.lights, 0,
+                 3, 0.001, self.wl.max_bounces)
         if self.batched:
             return tr.trace_views(self.views, ori, drs, *scene)
         return tr.trace(frame, self.t2w, ori, drs, *scene)
 
-    def trace_bwd(self, tr, fwd, pbr_grad, ray_ori=None, ray_dir=None, frame=0):
+    def trace_bwd(self, tr, fwd, pbr_grad, material_grad=None, ray_ori=None, ray_dir=None, frame=0, material=None,
+                  env=None):
         (rad, dns, hit, hit2, dist, nrm, snrm, mat, hits, vis, pbr, light, comps) = fwd
         z = self._zeros
         ori = self.ray_ori if ray_ori is None else ray_ori
         drs = self.ray_dir if ray_dir is None else ray_dir
-        args = (rad, dns, hit, hit2, dist, nrm, snrm, mat, pbr, light, self.density, self.material, self.sph, self.snrm,
-                self.env, self.alias, *self.lights, z["rad"], z["dns"], z["hit"], z["hit2"], z["dist"], z["nrm"],
-                z["snrm"], z["mat"], pbr_grad, z["light"], 0, 3, 0.001, self.wl.max_bounces)
+        args = (rad, dns, hit, hit2, dist, nrm, snrm, mat, pbr, light, self.density,
+                self.material if material is None else material, self.sph, self.snrm, self.env if env is None else env,
+                self.alias, *self.lights, z["rad"], z["dns"], z["hit"], z["hit2"], z["dist"], z["nrm"], z["snrm"],
+                z["mat"] if material_grad is None else material_grad, pbr_grad, z["light"], 0, 3, 0.001,
+                self.wl.max_bounces)
         if self.batched:
             return tr.trace_bwd_views(self.views, ori, drs, *args)
         return tr.trace_bwd(frame, self.t2w, ori, drs, *args)
@@ -295,6 +306,58 @@ def _view_config(views):
     return {"views": [list(v) for v in views]}
 
 
+# The loss of the timed training iteration: the terms of PTIR's default training loss
+# (configs/base_ptir.yaml:74-100, threedgrut/trainer.py:932-1125) that the tracer's outputs feed:
+# L1 on pred_pbr against the target render (lambda_l1 0.8), and the albedo and roughness prior
+# regularisations, L2 of pred_material against a prior image (lambda_init 0.5 and 0.2; the prior
+# here is the material image of the target scene). The prior terms give every primary interaction
+# a material gradient, so the adjoint re-traverses those segments even where no light reaches the
+# camera (the 1M-Gaussian scene's opaque shell keeps its pbr image black).
+LOSS_L1, LOSS_ALBEDO, LOSS_ROUGHNESS = 0.8, 0.5, 0.2
+STEP_DESC = ("lbvh refit + forward + loss (0.8 L1(pbr, target) + 0.5 L2(albedo, prior) + 0.2 L2(roughness, prior)) "
+             "+ adjoint + selective adam (material, env)")
+
+
+def loss_terms(pbr, material, target_pbr, prior_material):
+    """The iteration's loss and its gradients w.r.t. the per-sample pbr and material outputs."""
+    d = pbr - target_pbr
+    da = material[..., 0:3] - prior_material[..., 0:3]
+    dr = material[..., 3:4] - prior_material[..., 3:4]
+    loss = LOSS_L1 * d.abs().mean() + LOSS_ALBEDO * (da * da).mean() + LOSS_ROUGHNESS * (dr * dr).mean()
+    pbr_grad = torch.sign(d) * (LOSS_L1 / d.numel())
+    mat_grad = torch.zeros_like(material)
+    mat_grad[..., 0:3] = da * (2.0 * LOSS_ALBEDO / da.numel())
+    mat_grad[..., 3:4] = dr * (2.0 * LOSS_ROUGHNESS / dr.numel())
+    return loss, pbr_grad, mat_grad
+
+
+def loss_terms_np(pbr, material, target_pbr, prior_material):
+    """loss_terms() in numpy for the CPU legs: (pbr_grad, material_grad) float32."""
+    d = pbr.astype(np.float64) - target_pbr
+    da = material[..., 0:3].astype(np.float64) - prior_material[..., 0:3]
+    dr = material[..., 3:4].astype(np.float64) - prior_material[..., 3:4]
+    mat_grad = np.zeros(material.shape, np.float32)
+    mat_grad[..., 0:3] = da * (2.0 * LOSS_ALBEDO / da.size)
+    mat_grad[..., 3:4] = dr * (2.0 * LOSS_ROUGHNESS / dr.size)
+    return (np.sign(d) * (LOSS_L1 / d.size)).astype(np.float32), mat_grad
+
+
+def perturbed_material(material: torch.Tensor) -> torch.Tensor:
+    """The target scene's material: albedo + N(0, 0.02), seeded (the same bytes on every device)."""
+    gen = torch.Generator(device="cpu").manual_seed(1234)
+    mat_t = material.detach().cpu().clone()
+    mat_t[:, :3] += 0.02 * torch.randn(mat_t[:, :3].shape, generator=gen)
+    return mat_t.to(material.device)
+
+
+def bench_config(wl, args, world: int) -> dict:
+    """The `config` object shared by both arms (ours and the reference's CPU restatement)."""
+    return {"workload": wl.name, "storage": args.storage, "gaussians": wl.n, "views_per_gpu": len(wl.views),
+            **_view_config(wl.views), "max_bounces": wl.max_bounces, "env": list(wl.env_hw),
+            "step": (STEP_DESC if wl.backward else "lbvh refit + forward") + (" + grad all-reduce" if world > 1 else ""),
+            "parallelism": f"dp{world} over views"}
+
+
 def run_ours(args, rank, world, device):
     import torch.distributed as dist
 
@@ -312,47 +375,82 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, chunk_tiles=args.chunk_tiles)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
-    # target image: the same scene with albedo perturbed by N(0, 0.02)
-    gen = torch.Generator(device="cpu").manual_seed(1234)
-    mat_t = S.material.clone()
-    mat_t[:, :3] += (0.02 * torch.randn(mat_t[:, :3].shape, generator=gen)).to(device)
+    backward = S.wl.backward
     tr.build_bvh(S.pos, S.rot, S.scl, S.dns, True, True)
-    target = S.trace(tr, material=mat_t)[10].clone()
-    del mat_t
+    if backward:
+        # target image and material prior: the same scene with albedo perturbed by N(0, 0.02)
+        tgt = S.trace(tr, material=perturbed_material(S.material))
+        target, prior = tgt[10].clone(), tgt[7].clone()
+        del tgt
     torch.cuda.synchronize()
 
-    # optimizer state of the trained attributes: material [N,5] and environment [He,We,4]
-    adam = {k: (torch.zeros_like(t), torch.zeros_like(t)) for k, t in (("material", S.material), ("env", S.env))}
+    # the trained attributes, material [N,5] and environment [He,We,4], and their optimizer state
+    material = S.material.clone().requires_grad_(backward)
+    env = S.env.clone().requires_grad_(backward)
+    adam = {k: (torch.zeros_like(t), torch.zeros_like(t)) for k, t in (("material", material), ("env", env))}
+    # the step's ray inputs (device buffers, refilled from pinned host memory every timed step)
+    ori_d, dir_d = S.ray_ori.clone(), S.ray_dir.clone()
+    use_autograd = backward and not S.batched and not args.graph
+    if use_autograd:
+        from ptir_b200.tracer import LightBuffers, Tracer
 
-    def step(ray_ori=None, ray_dir=None, events=None, on_fwd=None, on_bwd=None):
-        """One training iteration: LBVH refit, forward, L1 loss gradient, adjoint, selective Adam."""
+        lights = LightBuffers(*S.lights)
+
+    def step(events=None, on_fwd=None, on_bwd=None):
+        """One training iteration: LBVH refit, forward, loss, adjoint, selective Adam. The eager
+        single-batch step goes through the reference-facing autograd entry (Tracer._Autograd: the
+        torch.autograd.Function of threedgptir_tracer/tracer.py:137-384) and loss.backward(); a
+        batch of views, or a step captured in a CUDA graph, calls trace / trace_bwd directly with
+        the same loss gradients."""
         tr.build_bvh(S.pos, S.rot, S.scl, S.dns, False, True)
         if events:
             events[0].record(stream)
-        fwd = S.trace(tr, ray_ori=ray_ori, ray_dir=ray_dir)
-        if events:
-            events[1].record(stream)
-        if on_fwd:
-            on_fwd()
-        pbr = fwd[10]
-        diff = pbr - target
-        loss = diff.abs().mean()
-        g = torch.sign(diff) * (1.0 / diff.numel())
-        if not hasattr(S, "_zeros"):
-            S.prepare_grads(fwd)
-        if events:
-            events[2].record(stream)
-        dg, mg, rg, sg, eg = S.trace_bwd(tr, fwd, g, ray_ori=ray_ori, ray_dir=ray_dir)
+        if not backward:
+            fwd = S.trace(tr, material=material, ray_ori=ori_d, ray_dir=dir_d)
+            if events:
+                events[1].record(stream)
+            if on_fwd:
+                on_fwd()
+            return fwd[10].mean()
+        if use_autograd:
+            out = Tracer._Autograd.apply(tr, 0, S.t2w, ori_d, dir_d, S.pos, S.rot, S.scl, S.dns, S.sph, S.snrm,
+                                         material[:, 0:3], material[:, 3:4], material[:, 4:5], env, S.alias, lights,
+                                         0, 3, 0.001, S.wl.max_bounces)
+            if events:
+                events[1].record(stream)
+            if on_fwd:
+                on_fwd()
+            loss = loss_terms(out[10], out[7], target, prior)[0]
+            if events:
+                events[2].record(stream)
+            loss.backward()
+            mg, eg, vis = material.grad, env.grad, out[9]
+        else:
+            fwd = S.trace(tr, material=material.detach(), ray_ori=ori_d, ray_dir=dir_d)
+            if events:
+                events[1].record(stream)
+            if on_fwd:
+                on_fwd()
+            loss, pbr_grad, mat_grad = loss_terms(fwd[10], fwd[7], target, prior)
+            if not hasattr(S, "_zeros"):
+                S.prepare_grads(fwd)
+            if events:
+                events[2].record(stream)
+            _, mg, _, _, eg = S.trace_bwd(tr, fwd, pbr_grad, material_grad=mat_grad, ray_ori=ori_d, ray_dir=dir_d,
+                                          material=material.detach(), env=env.detach())
+            vis = fwd[9]
         if events:
             events[3].record(stream)
         if on_bwd:
             on_bwd()
         if world > 1:
             pdist.allreduce_gradients([mg, eg])
-        visible = fwd[9].view(torch.int32) != 0
-        selective_adam_(S.material, mg, *adam["material"], visible, lr=ADAM_LR)
-        selective_adam_(S.env, eg, *adam["env"], None, lr=ADAM_LR)
-        return loss
+        with torch.no_grad():
+            selective_adam_(material, mg, *adam["material"], vis.view(torch.int32) != 0, lr=ADAM_LR)
+            selective_adam_(env, eg, *adam["env"], None, lr=ADAM_LR)
+        material.grad = None
+        env.grad = None
+        return loss.detach()
 
     # warm-up (also reads the deterministic per-launch counters, in total and per stage)
     got = {}
@@ -363,17 +461,17 @@ def run_ours(args, rank, world, device):
 
     for i in range(args.warmup):
         if i == 0:
-            step(on_fwd=lambda: read("fwd"), on_bwd=lambda: read("bwd"))
+            step(on_fwd=lambda: read("fwd"), on_bwd=(lambda: read("bwd")) if backward else None)
         else:
             step()
-    fc, bc, fcs, bcs = got["fwd"], got["bwd"], got["fwd_stages"], got["bwd_stages"]
+    zero = {k: 0 for k in got["fwd"]}
+    fc, fcs = got["fwd"], got["fwd_stages"]
+    bc, bcs = got.get("bwd", zero), got.get("bwd_stages", {st: zero for st in STAGES})
     torch.cuda.synchronize()
     status = tr.device_status()
     if status != 0:
         raise RuntimeError(f"device loop bound hit during warm-up (status {status})")
 
-    # the step's ray inputs: device buffers refilled from pinned host memory in the e2e loop
-    ori_d, dir_d = S.ray_ori.clone(), S.ray_dir.clone()
     graph, stage_t, stage_steps = None, None, args.steps
     if args.graph:
         if world > 1:
@@ -381,21 +479,26 @@ def run_ours(args, rank, world, device):
         # stage times of one eager step (no events can be recorded inside the graph), then the
         # whole iteration is captured once and replayed
         tr.stage_times()
-        step(ray_ori=ori_d, ray_dir=dir_d)
+        step()
         torch.cuda.synchronize()
         stage_t, stage_steps = tr.stage_times(), 1
         tr.set_collect_timings(False)
         side = torch.cuda.Stream()
         side.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(side):
-            step(ray_ori=ori_d, ray_dir=dir_d)
+            step()
         torch.cuda.current_stream().wait_stream(side)
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
-            graph_loss = step(ray_ori=ori_d, ray_dir=dir_d)
+            graph_loss = step()
         torch.cuda.synchronize()
 
-    # timed region, inputs resident in HBM
+    # Timed region: K steps. Every step copies its rays from pinned host memory into the input
+    # buffers and reads its loss back (the end-to-end figure, e2e); the step's own device time,
+    # inputs resident, is bracketed by events after the copy and before the read (value).
+    ori_h = S.ray_ori.cpu().pin_memory()
+    dir_h = S.ray_dir.cpu().pin_memory()
+    loss_h = torch.empty((args.steps,), dtype=torch.float32).pin_memory()
     clock_lines, stop = [], threading.Event()
     sampler = threading.Thread(target=_clock_sampler, args=(clock_lines, stop, torch.cuda.current_device()), daemon=True)
     sampler.start()
@@ -403,52 +506,40 @@ def run_ours(args, rank, world, device):
     if graph is None:
         tr.stage_times()  # forget the warm-up launches
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    s0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    s1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     t0.record(stream)
     for k in range(args.steps):
+        ori_d.copy_(ori_h, non_blocking=True)
+        dir_d.copy_(dir_h, non_blocking=True)
+        s0[k].record(stream)
         if graph is not None:
             graph.replay()
+            loss = graph_loss
         else:
-            step(events=ev[k])
+            loss = step(events=ev[k])
+        s1[k].record(stream)
+        loss_h[k:k + 1].copy_(loss.reshape(1), non_blocking=True)
     t1.record(stream)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     stop.set()
     sampler.join(timeout=10)
-    ms_total = t0.elapsed_time(t1)
+    e2e_ms = t0.elapsed_time(t1) / args.steps
+    ms_total = sum(a.elapsed_time(b) for a, b in zip(s0, s1))
+    if not all(math.isfinite(float(v)) for v in loss_h):
+        raise RuntimeError("non-finite loss in the timed steps")
     if graph is None:
         stage_t = tr.stage_times()  # {stage: (ms, launches)} over the timed steps
         fwd_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
-        bwd_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
+        bwd_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev) if backward else None
     else:
         fwd_ms = bwd_ms = None
-
-    # end to end through the public API with host buffers: rays H2D each step, loss D2H
-    ori_h = S.ray_ori.cpu().pin_memory()
-    dir_h = S.ray_dir.cpu().pin_memory()
-    e_steps = 1
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e_steps):
-        ori_d.copy_(ori_h, non_blocking=True)
-        dir_d.copy_(dir_h, non_blocking=True)
-        if graph is not None:
-            graph.replay()
-            loss = graph_loss
-        else:
-            loss = step(ray_ori=ori_d, ray_dir=dir_d)
-        loss_h = loss.to("cpu", non_blocking=True)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / e_steps
-    _ = float(loss_h)
     del graph
 
     status = tr.device_status()
@@ -456,13 +547,13 @@ def run_ours(args, rank, world, device):
         raise RuntimeError(f"device loop bound hit (status {status})")
 
     segs = fc["segments"]
-    stats = torch.tensor([ms_total, e2e_ms, float(segs)], dtype=torch.float64, device=device)
+    stats = torch.tensor([ms_total, e2e_ms * args.steps, float(segs)], dtype=torch.float64, device=device)
     if world > 1:
         mx = stats.clone()
         dist.all_reduce(mx, op=dist.ReduceOp.MAX)
         sm = stats.clone()
         dist.all_reduce(sm, op=dist.ReduceOp.SUM)
-        ms_total, e2e_ms, total_segs = float(mx[0]), float(mx[1]), float(sm[2])
+        ms_total, e2e_ms, total_segs = float(mx[0]), float(mx[1]) / args.steps, float(sm[2])
     else:
         total_segs = float(segs)
     if rank != 0:
@@ -480,8 +571,9 @@ def run_ours(args, rank, world, device):
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     launches_per_step = ACCEL_KERNELS_PER_BUILD + sum(n for _, n in stage_t.values()) / stage_steps
+    h2d = int(S.ray_ori.numel() * 4 * 2)
     res = {
-        "metric": METRIC,
+        "metric": metric_of(S.wl),
         "value": total_segs / (ms_step * 1e-3),
         "unit": "segments/s",
         "n_gpus": world,
@@ -493,14 +585,10 @@ def run_ours(args, rank, world, device):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": S.wl.name, "storage": args.storage, "gaussians": S.wl.n,
-                   "launch": shape or "defaults",
-                   "views_per_gpu": len(S.wl.views), **_view_config(S.wl.views),
-                   "max_bounces": S.wl.max_bounces, "env": list(S.wl.env_hw), "cuda_graph": bool(args.graph),
+        "config": {**bench_config(S.wl, args, world), "launch": shape or "defaults", "cuda_graph": bool(args.graph),
+                   "api": "Tracer._Autograd + loss.backward()" if use_autograd else "OptixTracer.trace / trace_bwd",
                    "samples_per_gpu": S.samples, "segments_per_step_per_gpu": segs,
-                   "step": "lbvh refit + forward + L1 loss grad + adjoint + selective adam (material, env)"
-                           + (" + grad all-reduce" if world > 1 else ""),
-                   "l2": "inputs larger than L2 (scene + BVH records ~400 MB)", "parallelism": f"dp{world} over views"},
+                   "l2": "inputs larger than L2 (scene + BVH records ~400 MB)"},
         "pass_ms": {"forward": fwd_ms, "backward": bwd_ms},
         "stages_ms_per_step": {KERNEL_OF_STAGE[st]: stage_t[st][0] / stage_steps for st in STAGES if stage_t[st][1]},
         "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom], "achieved": achieved, "peak": peak,
@@ -508,17 +596,22 @@ def run_ours(args, rank, world, device):
                      "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
                      "launches_per_step": launches_step},
         "counters": {"forward": fc, "backward": bc, "forward_by_stage": fcs, "backward_by_stage": bcs},
-        "e2e": {"value": total_segs / (e2e_ms * 1e-3), "unit": "segments/s",
-                "h2d_bytes_per_step": int(S.ray_ori.numel() * 4 * 2), "d2h_bytes_per_step": 4, "ms_per_step": e2e_ms},
+        "e2e": {"value": total_segs / (e2e_ms * 1e-3), "unit": "segments/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 4, "ms_per_step": e2e_ms, "steps": args.steps,
+                "timing": "the same K steps: rays copied from pinned host memory and the loss read back every step"},
         "gpu_launches": int(round(launches_per_step * args.steps)),
         "clocks": _clock_summary(clock_lines),
     }
     return res, S
 
 
-def cpu_sample(args, S=None, threads=0, budget_s=15.0):
+def cpu_sample(args, S=None, threads=0, budget_s=15.0, repeats=1):
     """Time the oracle's FP32 instantiation (the reference path restated on the CPU) on a bounded
-    sample of the workload: a block of rows of every view's first sample plane."""
+    sample of the workload: a block of rows of every view's first sample plane, forward and (for
+    workloads with a backward) the adjoint of the benchmark's loss. The loss's target render and
+    material prior (the same scene with perturbed albedo) are rendered by the oracle first, outside
+    the timed part. With `repeats` > 1 the sized sample is timed that many times and the value is
+    the median."""
     from oracle import oracle as O
 
     wl = workload_of(args)
@@ -527,27 +620,35 @@ def cpu_sample(args, S=None, threads=0, budget_s=15.0):
     alias = envmap.pack(envmap.build(env)).numpy()
     w, h, spp = wl.views[0]
     eyes = synthetic.camera_positions(len(wl.views), seed=wl.seed)
+    material = synthetic.material_tensor(f)
     base = dict(build_pos=f["pos"].numpy(), build_rot=f["rot"].numpy(), build_scl=f["scl"].numpy(),
                 build_dns=f["dns"].numpy(), density=synthetic.density_tensor(f).numpy(),
-                material=synthetic.material_tensor(f).numpy(), sph=f["sph"].numpy(), shading_normal=f["snrm"].numpy(),
+                material=material.numpy(), sph=f["sph"].numpy(), shading_normal=f["snrm"].numpy(),
                 environment=env.numpy(), alias_table=alias, ray_to_world=np.eye(4, dtype=np.float32)[None], frame=0,
                 sph_degree=3, min_transmittance=0.001, max_bounces=wl.max_bounces)
     cfg = O.OracleConfig()
+    jitter = synthetic.SPP_PATTERNS.get(spp, ((0.5, 0.5),))[0]
+    targets = {}
 
     def run(rows):
         oris, dirs = [], []
         for eye in eyes:
-            o, d = synthetic.pinhole_rays(w, h, eye)
+            o, d = synthetic.pinhole_rays(w, h, eye, jitter=jitter)
             r0 = (h - rows) // 2
             oris.append(o[r0:r0 + rows])
             dirs.append(d[r0:r0 + rows])
         s = dict(base, ray_ori=np.stack(oris), ray_dir=np.stack(dirs))
+        zhw = s["ray_ori"].shape[:3]
+        if wl.backward and rows not in targets:
+            targets[rows], _, _ = O.trace(cfg, dict(s, material=perturbed_material(material).numpy()), "f32",
+                                          threads=threads)
+        tgt = targets.get(rows)
         t = time.perf_counter()
         out, _, st = O.trace(cfg, s, "f32", threads=threads)
-        zhw = s["ray_ori"].shape[:3]
-        g = dict(pbr=np.full(zhw + (3,), 1.0 / np.prod(zhw), np.float32), light=np.zeros(zhw + (3,), np.float32),
-                 material=np.zeros(zhw + (5,), np.float32))
-        O.trace_bwd(cfg, s, out, g, "f32", threads=threads)
+        if wl.backward:
+            pbr_g, mat_g = loss_terms_np(out["pbr"], out["material"], tgt["pbr"], tgt["material"])
+            g = dict(pbr=pbr_g, light=np.zeros(zhw + (3,), np.float32), material=mat_g)
+            O.trace_bwd(cfg, s, out, g, "f32", threads=threads)
         return time.perf_counter() - t, st.segments, int(np.prod(zhw))
 
     rows = 2
@@ -556,10 +657,14 @@ def cpu_sample(args, S=None, threads=0, budget_s=15.0):
     if target_rows > rows:
         dt, segs, paths = run(target_rows)
         rows = target_rows
+    times = [dt] + [run(rows)[0] for _ in range(repeats - 1)]
+    dt = statistics.median(times)
     n_threads = threads or O.num_threads()
+    what = "fwd + adjoint of the benchmark loss" if wl.backward else "fwd"
     return {"value": segs / dt, "unit": "segments/s", "cores": n_threads, "kind": "port",
             "sample": f"{paths} paths ({len(eyes)} views x {rows} rows x {w} px, first sample of each pixel), "
-                      f"fwd+bwd oracle FP32, {dt:.1f} s", "seconds": dt, "segments": segs}
+                      f"{what}, oracle FP32, {dt:.1f} s (median of {len(times)})", "seconds": dt,
+            "segments": segs}
 
 
 def accuracy_sample(args, shape: dict, device, name: str = "field-300k-sh", res=(128, 96)) -> dict:
@@ -570,8 +675,17 @@ def accuracy_sample(args, shape: dict, device, name: str = "field-300k-sh", res=
     here: its background shell is opaque, so no light reaches the camera and its PBR image is
     black.) With 16-bit storage the oracle gets the attributes rounded as the tracer holds them.
     Both backward passes start from the oracle's forward values with the same seeded pbr
-    gradient."""
+    gradient.
+
+    The error is split by the paths' decision signatures (oracle/compare.py): "flipped" paths took
+    another discrete branch than the FP64 evaluation somewhere (and differ by whole
+    contributions), "agree" paths took the same branches. The gradients are reported for the
+    seeded gradient on every path ("grad_all") and with it zeroed on the flipped paths
+    ("grad_agree"). The oracle's own FP32 build, the same estimator in float32 on the CPU, is the
+    yardstick of float32's distance from FP64 ("oracle_fp32_vs_fp64")."""
+    from oracle import compare as K
     from oracle import oracle as O
+    from ptir_b200 import OptixTracer
 
     wl = synthetic.workload(name)
     f = synthetic.make_field(wl.n, seed=wl.seed, layout=wl.layout, scale_range=wl.scale_range, sh_full=wl.sh_full)
@@ -589,13 +703,9 @@ def accuracy_sample(args, shape: dict, device, name: str = "field-300k-sh", res=
     e = lambda *sh, dt=torch.float32: torch.empty(sh, dtype=dt, device=device)  # noqa: E731
     lights = (e(0, 9), e(5, 0), e(0, 3), e(0, 3, dt=torch.int32), e(0, 8), e(3, 0))
 
-    def rel_cos(a, b):
-        a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
-        nb = max(np.linalg.norm(b), 1e-30)
-        return float(np.linalg.norm(a - b) / nb), float(a @ b / max(np.linalg.norm(a) * nb, 1e-30))
-
     out = {"reference": "FP64 oracle, same sample sequences",
-           "sample": f"{wl.name} (config 4 scene): 1 view {w}x{h} at 1 spp, {wl.max_bounces} bounces"}
+           "sample": f"{wl.name} (config 4 scene): 1 view {w}x{h} at 1 spp, {wl.max_bounces} bounces",
+           "tolerance": f"per sample |x - ref| <= {K.TOL_ABS} + {K.TOL_REL} |ref|"}
     t0 = time.perf_counter()
     for storage, rnd in (("fp32", None), ("bf16", torch.bfloat16), ("fp16", torch.float16)):
         held = {k: (t if rnd is None else t.to(rnd).float()) for k, t in attrs.items()}
@@ -604,38 +714,41 @@ def accuracy_sample(args, shape: dict, device, name: str = "field-300k-sh", res=
                      max_bounces=wl.max_bounces, ray_ori=o[None].astype(np.float32), ray_dir=d[None].astype(np.float32))
         cfg = O.OracleConfig()
         ref, _, _ = O.trace(cfg, scene, "f64")
-        mg_ref, eg_ref, _ = O.trace_bwd(cfg, scene, ref, dict(pbr=g), "f64")
-        from ptir_b200 import OptixTracer
-
         tr = OptixTracer("", "", "reference", "referenceBwd", "instances", 4, 0.0113, True, 3, True, True, True,
                          False, False, storage=storage, **shape)
         tr.build_bvh(dev(f["pos"]), dev(f["rot"]), dev(f["scl"]), dev(f["dns"]), True, True)
         scene_t = (dev(attrs["density"]), dev(attrs["material"]), dev(f["sph"]), dev(f["snrm"]), e_env, e_alias,
                    *lights)
-        fwd = list(tr.trace(0, t2w, ori, drs, *scene_t, 0, 3, 0.001, wl.max_bounces))
+        sig_t = torch.zeros((1, h, w), dtype=torch.int32, device=device)
+        fwd = list(tr.trace(0, t2w, ori, drs, *scene_t, 0, 3, 0.001, wl.max_bounces, path_signature=sig_t))
         pbr = fwd[10].cpu().numpy()
+        sig = sig_t.cpu().numpy().view(np.uint32)
         fwd[10] = torch.from_numpy(ref["pbr"]).to(device)
         fwd[11] = torch.from_numpy(ref["light"]).to(device)
         z = torch.zeros_like
-        bw = tr.trace_bwd(0, t2w, ori, drs, *fwd[:8], fwd[10], fwd[11], *scene_t, z(fwd[0]), z(fwd[1]), z(fwd[2]),
-                          z(fwd[3]), z(fwd[4]), z(fwd[5]), z(fwd[6]), z(fwd[7]), torch.from_numpy(g).to(device),
-                          z(fwd[11]), 0, 3, 0.001, wl.max_bounces)
-        mg, eg = bw[1].cpu().numpy(), bw[4].cpu().numpy()
+
+        def gpu_bwd(grad):
+            bw = tr.trace_bwd(0, t2w, ori, drs, *fwd[:8], fwd[10], fwd[11], *scene_t, z(fwd[0]), z(fwd[1]),
+                              z(fwd[2]), z(fwd[3]), z(fwd[4]), z(fwd[5]), z(fwd[6]), z(fwd[7]),
+                              torch.from_numpy(grad).to(device), z(fwd[11]), 0, 3, 0.001, wl.max_bounces)
+            return bw[1].cpu().numpy(), bw[4].cpu().numpy()
+
+        g_m = K.masked_grad(g, sig, ref["path_sig"])
+        rep = K.image_report(pbr, ref["pbr"], sig, ref["path_sig"])
+        rep["grad_all"] = K.grad_report(*gpu_bwd(g), *O.trace_bwd(cfg, scene, ref, dict(pbr=g), "f64")[:2])
+        rep["grad_agree"] = K.grad_report(*gpu_bwd(g_m), *O.trace_bwd(cfg, scene, ref, dict(pbr=g_m), "f64")[:2])
         if storage == "fp32":
             # yardstick: the same estimator in float32 on the CPU (the oracle's FP32 instantiation)
             r32, _, _ = O.trace(cfg, scene, "f32")
-            e32 = np.abs(r32["pbr"].astype(np.float64) - ref["pbr"].astype(np.float64))
-            out["oracle_fp32_vs_fp64"] = {
-                "pbr_within_1e-3": round(float(np.all(e32 <= 1e-3 + 1e-3 * np.abs(ref["pbr"]), axis=-1).mean()), 5),
-                "pbr_rel_l2": rel_cos(r32["pbr"], ref["pbr"])[0], "pbr_max_abs": float(e32.max())}
-        err = np.abs(pbr.astype(np.float64) - ref["pbr"].astype(np.float64))
-        ok = np.all(err <= 1e-3 + 1e-3 * np.abs(ref["pbr"]), axis=-1)
-        m_rel, m_cos = rel_cos(mg[:, :4], mg_ref[:, :4])
-        e_rel, e_cos = rel_cos(eg[..., :3], eg_ref[..., :3])
-        out[storage] = {"pbr_within_1e-3": round(float(ok.mean()), 5), "pbr_max_abs": float(err.max()),
-                        "pbr_mean_abs": float(err.mean()), "pbr_rel_l2": rel_cos(pbr, ref["pbr"])[0],
-                        "material_grad_rel_l2": m_rel, "material_grad_cos": m_cos,
-                        "env_grad_rel_l2": e_rel, "env_grad_cos": e_cos}
+            y = K.image_report(r32["pbr"], ref["pbr"], r32["path_sig"], ref["path_sig"])
+            g32 = K.masked_grad(g, r32["path_sig"], ref["path_sig"])
+            y["grad_all"] = K.grad_report(*O.trace_bwd(cfg, scene, ref, dict(pbr=g), "f32")[:2],
+                                          *O.trace_bwd(cfg, scene, ref, dict(pbr=g), "f64")[:2])
+            y["grad_agree"] = K.grad_report(*O.trace_bwd(cfg, scene, ref, dict(pbr=g32), "f32")[:2],
+                                            *O.trace_bwd(cfg, scene, ref, dict(pbr=g32), "f64")[:2])
+            out["oracle_fp32_vs_fp64"] = y
+            out["gpu_fp32_vs_oracle_fp32"] = K.image_report(pbr, r32["pbr"], sig, r32["path_sig"])
+        out[storage] = rep
         del tr
     out["seconds"] = round(time.perf_counter() - t0, 1)
     return out
@@ -676,22 +789,22 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        samples = [cpu_sample(args, budget_s=10.0) for _ in range(max(1, args.steps))]
-        v = statistics.median(s["value"] for s in samples)
+        # one bounded sample sized to ~budget seconds, timed once per step (median)
+        steps = max(1, args.steps)
+        base = cpu_sample(args, budget_s=max(3.0, min(10.0, 150.0 / steps)), repeats=steps)
+        v = base["value"]
         wl = workload_of(args)
-        w, h, spp = wl.views[0]
-        base = samples[0]
         print(json.dumps({
-            "impl": "reference", "metric": METRIC, "value": v, "unit": "segments/s", "n_gpus": args.gpus,
+            "impl": "reference", "metric": metric_of(wl), "value": v, "unit": "segments/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl.name, "gaussians": wl.n, "views_per_gpu": len(wl.views),
-                       **_view_config(wl.views), "max_bounces": wl.max_bounces},
+            "config": dict(bench_config(wl, args, world), storage="fp32"),
             "cpu_baseline": {"value": v, "unit": "segments/s", "cores": base["cores"], "kind": "port",
                              "sample": base["sample"]},
             "e2e": {"value": v, "unit": "segments/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's OptiX tracer cannot be built here (OptiX SDK headers absent); its per-ray "
-                    "math restated in C++ (oracle/oracle.cpp) runs on the host cores instead",
+                    "math restated in C++ (oracle/oracle.cpp) runs on the host cores instead, in FP32 (the "
+                    "reference's arithmetic and storage)",
         }))
         return
 

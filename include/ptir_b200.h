@@ -15,11 +15,19 @@
  *                       message is kept on the handle.
  *
  * Conventions
- *   - Every pointer named in an args struct is DEVICE memory, float32, C-contiguous, in the
- *     reference's tensor layout; the caller owns all of it (inputs and outputs), as torch does
- *     for the reference (optixTracer.cpp:931-944, 1057-1063). Output buffers need no
- *     initialisation: every element is written (the reference's zero-filled outputs are
- *     written as zeros).
+ *   - Every pointer named in an args struct is DEVICE memory, float32, in the reference's tensor
+ *     layout; the caller owns all of it (inputs and outputs), as torch does for the reference
+ *     (optixTracer.cpp:931-944, 1057-1063). Particle, environment and light tables and every
+ *     output are C-contiguous (the reference passes them through getPtr, a contiguous copy,
+ *     tensorBuffering.h:30-39). The per-sample inputs (ray origins and directions, and the
+ *     backward's saved outputs and incoming gradients) may be strided, as the reference reads
+ *     them through PackedTensorAccessor32 (tensorBuffering.h:41-45, optixTracer.cpp:963-964,
+ *     1082-1113): each has a `*_strides[4]` field, the element strides of its [Z,H,W,C] index
+ *     (z, y, x, c), any of them 0 for a broadcast dimension; all four 0 means C-contiguous. In
+ *     the batched entry points (ptir_trace_views) the per-sample arrays are flat [T,C]: element
+ *     (t, c) lies at t * strides[2] + c * strides[3], strides[0] and [1] are unused. Output
+ *     buffers need no initialisation: every element is written (the reference's zero-filled
+ *     outputs are written as zeros).
  *   - The library owns its acceleration structure and scratch; buffers grow, never shrink.
  *   - All work is enqueued on `stream` (a cudaStream_t); no entry point synchronises the host
  *     with the device, so a trace can be captured in a CUDA graph once the structure exists.
@@ -35,7 +43,7 @@
 extern "C" {
 #endif
 
-#define PTIR_ABI_VERSION 3
+#define PTIR_ABI_VERSION 4
 
 enum {
     PTIR_OK = 0,
@@ -136,6 +144,8 @@ typedef struct ptir_trace_args {
     int32_t sph_eval_degree;        /* SH degree evaluated (<= sph_degree) */
     float min_transmittance;        /* render.min_transmittance */
     uint32_t max_bounces;           /* render.max_bounces */
+    int64_t ray_origin_strides[4];    /* element strides of ray_origin (see Conventions); 0s: contiguous */
+    int64_t ray_direction_strides[4]; /* element strides of ray_direction */
 } ptir_trace_args;
 
 /* Forward outputs, [Z,H,W,C] (optixTracer.cpp:931-944). */
@@ -154,6 +164,12 @@ typedef struct ptir_trace_outputs {
     float* pbr_components;             /* [Z,H,W,2,3] direct / indirect */
     float* visibility;                 /* [N,1]: int32 1 stored in the float32 element per visible Gaussian;
                                           cleared by the call */
+    uint32_t* path_signature;          /* [Z,H,W] or NULL (no counterpart in the reference): per path an FNV-1a
+                                          hash of its discrete decisions in path order (each segment's
+                                          accepted-hit count, interaction and escape flags; NEE shadow ray
+                                          cast and occluded; continuation after each BRDF sample). Two
+                                          evaluations of a path with equal signatures took the same branches;
+                                          the oracle computes the same hash. */
 } ptir_trace_outputs;
 
 /* Backward inputs: the saved forward outputs and the gradients flowing into them
@@ -164,6 +180,8 @@ typedef struct ptir_bwd_args {
     const float* pbr_grad;        /* [Z,H,W,3] */
     const float* light_grad;      /* [Z,H,W,3] */
     const float* material_grad;   /* [Z,H,W,5] */
+    /* element strides of the five arrays above (see Conventions); all 0: contiguous */
+    int64_t pbr_strides[4], light_strides[4], pbr_grad_strides[4], light_grad_strides[4], material_grad_strides[4];
 } ptir_bwd_args;
 
 /* Backward outputs. The reference's backward fills only the material and environment

@@ -158,6 +158,13 @@ struct Pending {  // payLoad.h:97-138
 template <class T>
 struct Path {  // payLoad.h:140-168
     unsigned active = 1, bounces = 0, max_bounces = 0;
+    // Decision signature (no counterpart in the reference; for parity diagnostics): an FNV-1a hash
+    // over the events in which a path takes a discrete branch, in path order, computed the same
+    // way by the GPU tracer (path.cuh, sig_*): each segment's accepted-hit count, interaction,
+    // escape and hit flags; whether NEE casts a shadow ray and whether it is occluded; whether the
+    // path continues after each BRDF sample.
+    uint32_t sig = 2166136261u;
+    void mix(uint32_t v) { sig = (sig ^ v) * 16777619u; }
     RayPayload<T> cur{}, emitter{};
     V3<T> acc{}, acc_grad{}, acc_direct{}, acc_indirect{}, acc_light{}, acc_light_grad{};
     V3<T> throughput = v3<T>(T(1));
@@ -412,7 +419,7 @@ public:
                     if (visibility) visibility[h.id] = 1.0f;
                 }
                 p.last_hit = std::fmax(p.last_hit, T(h.t));
-                if (cfg.enable_hitcounts) p.hits_count += accept ? T(1) : T(0);
+                p.hits_count += accept ? T(1) : T(0);  // output only with enable_hitcounts
             }
         }
         const T op = T(1) - p.transmittance;
@@ -1138,8 +1145,12 @@ public:
         const LightSample ls = sample_light(it.position, s);
         const T lpdf = ls.pdf;
         const V3<T> wi = ls.wi, Li = ls.Li;
-        if (lpdf <= T(0) || is_zero(Li)) { P.emitter = RayPayload<T>(); return; }
-        if (dot(it.snormal, wi) <= T(0)) { P.emitter = RayPayload<T>(); return; }
+        if (lpdf <= T(0) || is_zero(Li) || dot(it.snormal, wi) <= T(0)) {
+            P.emitter = RayPayload<T>();
+            P.mix(kSigNee);
+            return;
+        }
+        P.mix(kSigNee | 1u);
         V3<T> n, wo, alb; T met;
         frame_of(it, P.cur.ray.d, n, wo, alb, met);
         const V3<T> bc = eval_brdf(wo, n, alb, met, clamp_rough(it.roughness), wi, spdf);
@@ -1147,7 +1158,9 @@ public:
         const Ray<T> lr{it.position + wi * T(2e-2), wi};
         const T tmax = ls.dist < T(1e19) ? std::fmax(T(0), ls.dist - T(2e-2)) : T(1e20);
         st.segments++;
-        if (shadow_occluded(lr, s, T(0), tmax)) { P.emitter = RayPayload<T>(); return; }
+        const bool occluded = shadow_occluded(lr, s, T(0), tmax);
+        P.mix(kSigShadow | (occluded ? 1u : 0u));
+        if (occluded) { P.emitter = RayPayload<T>(); return; }
         P.emitter = RayPayload<T>(lr, T(0));
         P.emitter.light_pdf = lpdf;
         P.emitter.scatter_pdf = spdf;
@@ -1393,6 +1406,12 @@ public:
         return r;
     }
 
+    static uint32_t sig_segment(const RayPayload<T>& p) {
+        const double hc = std::fmin(std::fmax(double(p.hits_count), 0.0), 65535.0);
+        return uint32_t(hc) | (p.inter.valid ? 1u << 16 : 0u) | (p.valid ? 1u << 17 : 0u) | (p.hit ? 1u << 18 : 0u);
+    }
+    static constexpr uint32_t kSigNee = 0x100000u, kSigShadow = 0x200000u, kSigCont = 0x300000u;
+
     unsigned max_bounces() const {  // optixTracer.cpp:959
         return in.render_opts ? std::min(in.max_bounces, 2u) : in.max_bounces;
     }
@@ -1406,6 +1425,8 @@ public:
         const Ray<T> ray = world_ray(li);
         st.segments++;
         ray_intersect(false, ray, P.cur, s);
+        P.mix(sig_segment(P.cur));
+        if (out.path_sig) out.path_sig[li] = P.sig;
         // pathTracer.cuh:636-663
         auto put = [](float* dst, size_t li, int c, std::initializer_list<T> v) {
             if (!dst) return;
@@ -1438,10 +1459,14 @@ public:
             if (!P.active) break;
             P.bounces = depth + 1u;
             sample_next(P, s);
-            if (vmax(P.throughput) < T(1e-4)) break;
+            const bool cont = P.active && !(vmax(P.throughput) < T(1e-4));
+            P.mix(kSigCont | (cont ? 1u : 0u));
+            if (!cont) break;
             st.segments++;
             ray_intersect(true, P.cur.ray, P.cur, s);
+            P.mix(sig_segment(P.cur));
         }
+        if (out.path_sig) out.path_sig[li] = P.sig;
         // pathTracer.cuh:665-681
         put(out.pbr, li, 3, {P.acc.x, P.acc.y, P.acc.z});
         put(out.light, li, 3, {P.acc_light.x, P.acc_light.y, P.acc_light.z});
@@ -1528,6 +1553,7 @@ struct orc_scene {
 struct orc_fwd_out {
     float *radiance, *density, *hit, *hit2, *distortion, *normal, *snormal, *material, *hits_count, *pbr, *light,
         *components, *visibility;
+    uint32_t* path_sig;
 };
 
 struct orc_bwd_in {
@@ -1598,6 +1624,7 @@ static int run_fwd(const orc_config* c, const orc_scene* s, const orc_fwd_out* o
     out.radiance = o->radiance; out.density = o->density; out.hit = o->hit; out.hit2 = o->hit2;
     out.distortion = o->distortion; out.normal = o->normal; out.snormal = o->snormal; out.material = o->material;
     out.hits_count = o->hits_count; out.pbr = o->pbr; out.light = o->light; out.components = o->components;
+    out.path_sig = o->path_sig;
     if (o->visibility) std::fill(o->visibility, o->visibility + in.n, 0.0f);
     const long long total = (long long)in.nz * in.h * in.w;
     if (stride < 1) stride = 1;

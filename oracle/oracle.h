@@ -193,6 +193,7 @@ struct FwdOut {
           *normal = nullptr, *snormal = nullptr, *material = nullptr, *hits_count = nullptr, *pbr = nullptr,
           *light = nullptr, *components = nullptr;  // components [nz,h,w,2,3]
     float* visibility = nullptr;                    // [n] (1.0 where any accepted hit)
+    uint32_t* path_sig = nullptr;                   // [nz,h,w] decision signature of each path
 };
 
 // backward inputs (the saved forward outputs plus their gradients) and outputs

@@ -63,7 +63,7 @@ class _Scene(C.Structure):
 class _FwdOut(C.Structure):
     _fields_ = [(k, _FP) for k in (
         "radiance", "density", "hit", "hit2", "distortion", "normal", "snormal", "material",
-        "hits_count", "pbr", "light", "components", "visibility")]
+        "hits_count", "pbr", "light", "components", "visibility")] + [("path_sig", C.POINTER(C.c_uint32))]
 
 
 class _BwdIn(C.Structure):
@@ -217,14 +217,17 @@ _FWD_CH = {"radiance": 3, "density": 1, "hit": 2, "hit2": 1, "distortion": 1, "n
 
 
 def trace(cfg: OracleConfig, scene: dict, precision: str = "f64", threads: int = 0, stride: int = 1):
-    """Forward trace. Returns (dict of outputs [nz,h,w,C] float32, visibility [n], Stats)."""
+    """Forward trace. Returns (dict of outputs [nz,h,w,C] float32, visibility [n], Stats); the
+    dict also holds 'path_sig' [nz,h,w] uint32, each path's decision signature (the hash the GPU
+    tracer writes to its path_signature output)."""
     keep = _Keep()
     sc = _scene(keep, scene)
     shape = (sc.nz, sc.h, sc.w)
     outs = {k: np.zeros(shape + (_FWD_CH[k],), np.float32) for k in FWD_KEYS}
     outs["components"] = outs["components"].reshape(shape + (2, 3))
     vis = np.zeros((max(sc.n, 1),), np.float32)
-    fo = _FwdOut(*[_f(outs[k]) for k in FWD_KEYS], _f(vis))
+    sig = np.zeros(shape, np.uint32)
+    fo = _FwdOut(*[_f(outs[k]) for k in FWD_KEYS], _f(vis), sig.ctypes.data_as(C.POINTER(C.c_uint32)))
     st = Stats()
     c = cfg._c()
     if precision == "f64":
@@ -233,6 +236,7 @@ def trace(cfg: OracleConfig, scene: dict, precision: str = "f64", threads: int =
     else:
         rc = lib().orc_trace_f32(C.byref(c), C.byref(sc), C.byref(fo), threads, stride, C.byref(st))
     assert rc == 0
+    outs["path_sig"] = sig
     return outs, vis[: sc.n], st
 
 

@@ -11,6 +11,7 @@ from . import build as _build
 
 _LIB = None
 
+ABI_VERSION = 4  # PTIR_ABI_VERSION of include/ptir_b200.h that these structs mirror
 PTIR_OK = 0
 PTIR_EINVAL = 1
 PTIR_ECUDA = 2
@@ -90,17 +91,21 @@ class PtirTraceArgs(C.Structure):
         ("sph_eval_degree", C.c_int32),
         ("min_transmittance", C.c_float),
         ("max_bounces", C.c_uint32),
+        ("ray_origin_strides", C.c_int64 * 4),
+        ("ray_direction_strides", C.c_int64 * 4),
     ]
 
 
 class PtirTraceOutputs(C.Structure):
     _fields_ = [(k, _FP) for k in (
         "radiance", "density", "hit_distance", "hit_distance_second_moment", "depth_distortion", "normal",
-        "shading_normal", "material", "hits_count", "pbr", "light", "pbr_components", "visibility")]
+        "shading_normal", "material", "hits_count", "pbr", "light", "pbr_components", "visibility",
+        "path_signature")]
 
 
 class PtirBwdArgs(C.Structure):
-    _fields_ = [(k, _FP) for k in ("pbr", "light", "pbr_grad", "light_grad", "material_grad")]
+    _fields_ = [(k, _FP) for k in ("pbr", "light", "pbr_grad", "light_grad", "material_grad")] + [
+        (k + "_strides", C.c_int64 * 4) for k in ("pbr", "light", "pbr_grad", "light_grad", "material_grad")]
 
 
 class PtirBwdOutputs(C.Structure):
@@ -140,6 +145,9 @@ def load(build_if_missing: bool = True):
     L = C.CDLL(path)
     P = C.POINTER
     L.ptir_abi_version.restype = C.c_int
+    if L.ptir_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{path} has ABI version {L.ptir_abi_version()}, these bindings need {ABI_VERSION}: "
+                           "rebuild it (python -m ptir_b200.build)")
     L.ptir_create.argtypes = [P(PtirConfig), P(C.c_void_p)]
     L.ptir_create.restype = C.c_int
     L.ptir_destroy.argtypes = [C.c_void_p]

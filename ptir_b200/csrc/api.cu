@@ -109,12 +109,31 @@ unsigned flags_of(const ptir_config& c) {
     return f;
 }
 
-// checks shared by trace and trace_bwd; fills the kernel parameters
+// Element strides of a per-sample array from the caller's (all zero: C-contiguous with `channels`
+// channels); false for a negative stride. `flat`: the batched [T,C] form, where only the sample
+// stride (strides[2]) and the channel stride (strides[3]) apply.
+bool sample_layout(const int64_t* s, int channels, int h, int w, bool flat, ptir::SampleLayout& L) {
+    if (s[0] == 0 && s[1] == 0 && s[2] == 0 && s[3] == 0) {
+        L.sc = 1;
+        L.sx = channels;
+        L.sy = flat ? 0 : (long long)channels * w;
+        L.sz = flat ? 0 : (long long)channels * w * h;
+        return true;
+    }
+    if (s[0] < 0 || s[1] < 0 || s[2] < 0 || s[3] < 0) return false;
+    L.sz = flat ? 0 : s[0];
+    L.sy = flat ? 0 : s[1];
+    L.sx = s[2];
+    L.sc = s[3];
+    return true;
+}
+
 // checks shared by every trace entry point; fills the kernel parameters and the launch count.
 // `views` null: the single launch of the reference (args' extent, frame and ray_to_world).
 int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, int nviews, ptir::TraceParams& p,
             long long& launches) {
     if (!a) return fail(t, PTIR_EINVAL, "null trace arguments");
+    const bool flat = views != nullptr;
     ptir_view single;
     if (!views) {
         single.z = a->z;
@@ -206,6 +225,10 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, in
     p.lights.tri_cols = a->mesh_light_alias_cols;
     p.ray_ori = a->ray_origin;
     p.ray_dir = a->ray_direction;
+    p.flat_samples = flat ? 1 : 0;
+    if (!sample_layout(a->ray_origin_strides, 3, a->h, a->w, flat, p.ray_ori_layout) ||
+        !sample_layout(a->ray_direction_strides, 3, a->h, a->w, flat, p.ray_dir_layout))
+        return fail(t, PTIR_EINVAL, "negative ray stride");
     long long offset = 0, tile0 = 0;
     for (int v = 0; v < nviews; ++v) {
         const ptir_view& V = views[v];
@@ -396,6 +419,8 @@ int trace_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views,
     fo.light = o->light;
     fo.components = o->pbr_components;
     fo.visibility = o->visibility;
+    fo.path_sig = o->path_signature;
+    if (o->path_signature) p.flags |= ptir::kPathSig;
     const ptir::StageCtx sc = stage_ctx(t);
     e = t->cfg.schedule == PTIR_SCHEDULE_MEGAKERNEL
             ? ptir::launch_trace_fwd(p, fo, sc, s)
@@ -436,6 +461,13 @@ int trace_bwd_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* vi
     bi.pbr_grad = b->pbr_grad;
     bi.light_grad = b->light_grad;
     bi.material_grad = b->material_grad;
+    const bool flat = views != nullptr;
+    if (!sample_layout(b->pbr_strides, 3, a->h, a->w, flat, bi.pbr_layout) ||
+        !sample_layout(b->light_strides, 3, a->h, a->w, flat, bi.light_layout) ||
+        !sample_layout(b->pbr_grad_strides, 3, a->h, a->w, flat, bi.pbr_grad_layout) ||
+        !sample_layout(b->light_grad_strides, 3, a->h, a->w, flat, bi.light_grad_layout) ||
+        !sample_layout(b->material_grad_strides, 5, a->h, a->w, flat, bi.material_grad_layout))
+        return fail(t, PTIR_EINVAL, "negative stride of a backward input");
     bi.particle_material_grad = o->particle_material_grad;
     bi.environment_grad = env ? o->environment_grad : nullptr;
     // compensation buffers of the Kahan-pair gradient sums: [n,5] then [eh,ew,4], zeroed per call

@@ -44,6 +44,7 @@ enum Flags : unsigned {
     kVisualizeLights = 16u,
     kExactReplay = 32u,  // backward re-traversals include the segment's last composited Gaussian
     kWarpAggregate = 64u,  // gradient rows shared by lanes of a warp are summed before the atomics
+    kPathSig = 128u,       // keep a per-path signature of the path's discrete decisions (FwdOutputs::path_sig)
 };
 
 // Punctual and area lights: the reference's LightBuffers (threedgptir_tracer/tracer.py:40-119),
@@ -87,13 +88,28 @@ struct ViewDesc {
 
 constexpr int kMaxViews = 64;  // views of one batch (passed by value with the kernel parameters)
 
+// Element strides of a per-sample array (PackedTensorAccessor32 semantics): element (z, y, x, c)
+// of a [Z,H,W,C] launch array at z*sz + y*sy + x*sx + c*sc; in a batch of views the arrays are
+// flat [T,C] and sample t (the flat launch index) lies at t*sx + c*sc.
+struct SampleLayout {
+    long long sz, sy, sx, sc;
+};
+
+// offset of channel 0 of a sample: (z, y, x) within its launch, li its flat index in the batch
+__device__ __forceinline__ long long sample_offset(const SampleLayout& L, bool flat, unsigned z, unsigned y,
+                                                   unsigned x, size_t li) {
+    return flat ? (long long)li * L.sx : (long long)z * L.sz + (long long)y * L.sy + (long long)x * L.sx;
+}
+
 struct TraceParams {
     AccelView accel;
     ParticleView part;
     EnvView env;
     LightView lights;
-    const float* ray_ori;        // [z, h, w, 3]
+    const float* ray_ori;        // [z, h, w, 3], strided (ray_ori_layout)
     const float* ray_dir;
+    SampleLayout ray_ori_layout, ray_dir_layout;
+    int flat_samples;            // 1: per-sample arrays are flat [T,C] over the batch of views
     ViewDesc views[kMaxViews];   // the launches of this trace (one for the reference's single launch)
     int nviews;
     long long tiles;             // 8x4 pixel tiles of all views
@@ -123,14 +139,16 @@ struct FwdOutputs {
     float* light;       // [z,h,w,3]
     float* components;  // [z,h,w,2,3]
     float* visibility;  // [n] float32 tensor holding int32 1 where an accepted hit occurred
+    unsigned* path_sig; // [z,h,w] decision signature of each path (kPathSig), or null
 };
 
 struct BwdInputs {
-    const float* pbr;            // [z,h,w,3]
+    const float* pbr;            // [z,h,w,3], strided (pbr_layout)
     const float* light;          // [z,h,w,3]
     const float* pbr_grad;       // [z,h,w,3]
     const float* light_grad;     // [z,h,w,3]
     const float* material_grad;  // [z,h,w,5]
+    SampleLayout pbr_layout, light_layout, pbr_grad_layout, light_grad_layout, material_grad_layout;
     float* particle_material_grad;  // [n,5]
     float* environment_grad;        // [eh,ew,4]
     float* particle_material_comp;  // [n,5] compensation terms of the material gradient sums, or null

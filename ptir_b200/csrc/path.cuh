@@ -52,6 +52,7 @@ struct Emitter {
 
 struct PathState {
     unsigned active, bounces, max_bounces;
+    unsigned sig;  // decision signature (kPathSig): FNV-1a over the path's discrete events
     float3 acc, acc_grad, acc_direct, acc_indirect, acc_light, acc_light_grad, throughput;
     Emitter em;
     // pending roughness gradient through the next direction (payLoad.h:97-138)
@@ -226,11 +227,28 @@ PTIR_DEV void emitter_clear(Emitter& em) {
     em.tmax = kFarT;
 }
 
+// ------------------------------------------------------------------------------------
+// Decision signature of a path (diagnostics, P.flags & kPathSig): an FNV-1a hash over the events
+// in which a float evaluation takes a discrete branch, in path order: per segment its accepted-hit
+// count, interaction and escape flags; whether NEE casts a shadow ray and whether it is occluded;
+// whether the path continues after each BRDF sample. Two evaluations of the same path (this
+// tracer and the oracle, or two precisions) with equal signatures took the same branches.
+PTIR_DEV unsigned sig_mix(unsigned h, unsigned v) { return (h ^ v) * 16777619u; }
+PTIR_DEV unsigned sig_segment(const Segment& s) {
+    const unsigned hits = (unsigned)fminf(fmaxf(s.hits_count, 0.0f), 65535.0f);
+    return hits | (s.ivalid ? 1u << 16 : 0u) | (s.escaped ? 1u << 17 : 0u) | (s.hit ? 1u << 18 : 0u);
+}
+constexpr unsigned kSigNee = 0x100000u, kSigShadow = 0x200000u, kSigCont = 0x300000u;
+PTIR_DEV void sig_event(const TraceParams& P, PathState& ps, unsigned v) {
+    if (P.flags & kPathSig) ps.sig = sig_mix(ps.sig, v);
+}
+PTIR_DEV bool path_continues(const PathState& ps) { return ps.active && !(max3(ps.throughput) < 1e-4f); }
+
 // Next-event estimation (pathTracer.cuh:461-504), first half: light sample, visibility-independent
 // checks and BRDF. Fills the emitter as if unoccluded and returns true when a shadow ray has to
 // decide it (nee_shadow).
 template <class Ctx>
-PTIR_DEV bool nee_prepare(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
+PTIR_DEV bool nee_prepare_light(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
     const TraceParams& P = C.P;
     emitter_clear(ps.em);
     const LightSample ls = sample_light(P, s.pos, rng, C.ctr.env);
@@ -254,13 +272,22 @@ PTIR_DEV bool nee_prepare(const Ctx& C, PathState& ps, const Segment& s, Pcg32& 
     return true;
 }
 
+template <class Ctx>
+PTIR_DEV bool nee_prepare(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
+    const bool shadow = nee_prepare_light(C, ps, s, rng);
+    sig_event(C.P, ps, kSigNee | (shadow ? 1u : 0u));
+    return shadow;
+}
+
 // second half: the stochastic shadow ray from the interaction toward the sampled direction;
 // an occluded sample leaves an empty emitter
 template <class Ctx>
 PTIR_DEV void nee_shadow(const Ctx& C, PathState& ps, const Segment& s, Pcg32& rng) {
     ++C.ctr.segments;
     const float3 wi = ps.em.dir;
-    if (shadow_occluded(C, s.pos + wi * 2e-2f, wi, ps.em.tmax, rng)) emitter_clear(ps.em);
+    const bool occluded = shadow_occluded(C, s.pos + wi * 2e-2f, wi, ps.em.tmax, rng);
+    sig_event(C.P, ps, kSigShadow | (occluded ? 1u : 0u));
+    if (occluded) emitter_clear(ps.em);
 }
 
 template <class Ctx>
@@ -361,6 +388,7 @@ PTIR_DEV void accumulate_light(const Ctx& C, PathState& ps, Segment& s) {
 }
 
 PTIR_DEV void path_init(PathState& ps, unsigned max_bounces) {
+    ps.sig = 2166136261u;
     ps.active = 1u;
     ps.bounces = 0u;
     ps.max_bounces = max_bounces;
@@ -374,12 +402,45 @@ PTIR_DEV void path_init(PathState& ps, unsigned max_bounces) {
     ps.pend_bounces = 0u;
 }
 
-PTIR_DEV void world_ray(const TraceParams& P, int view, size_t li, float3& o, float3& d) {
+// channels 0..2 of a strided per-sample array at element offset `off`
+PTIR_DEV float3 ld_sample3(const float* a, const SampleLayout& L, long long off) {
+    return make_float3(__ldg(a + off), __ldg(a + off + L.sc), __ldg(a + off + 2 * L.sc));
+}
+
+// world-space ray of sample (x, y, z) of launch `view` (flat index li)
+PTIR_DEV void world_ray(const TraceParams& P, int view, unsigned x, unsigned y, unsigned z, size_t li, float3& o,
+                        float3& d) {
     const float* m = P.views[view].to_world;
-    const float3 lo = ld3(P.ray_ori + 3 * li), ld = ld3(P.ray_dir + 3 * li);
+    const bool flat = P.flat_samples != 0;
+    const float3 lo = ld_sample3(P.ray_ori, P.ray_ori_layout, sample_offset(P.ray_ori_layout, flat, z, y, x, li));
+    const float3 ld = ld_sample3(P.ray_dir, P.ray_dir_layout, sample_offset(P.ray_dir_layout, flat, z, y, x, li));
     const float3 m0 = ld3(m), m1 = ld3(m + 4), m2 = ld3(m + 8);
     o = make_float3(dot(m0, lo) + __ldg(m + 3), dot(m1, lo) + __ldg(m + 7), dot(m2, lo) + __ldg(m + 11));
     d = make_float3(dot(m0, ld), dot(m1, ld), dot(m2, ld));
+}
+
+// The adjoint's per-sample inputs (the forward's pbr and light and their incoming gradients) into
+// the path state, and the incoming material-output gradient onto the primary interaction.
+PTIR_DEV void load_adjoint_inputs(const TraceParams& P, const BwdInputs& B, unsigned x, unsigned y, unsigned z,
+                                  size_t li, PathState& ps) {
+    const bool flat = P.flat_samples != 0;
+    auto at = [&](const float* a, const SampleLayout& L) {
+        return a ? ld_sample3(a, L, sample_offset(L, flat, z, y, x, li)) : f3(0.0f);
+    };
+    ps.acc = at(B.pbr, B.pbr_layout);
+    ps.acc_grad = at(B.pbr_grad, B.pbr_grad_layout);
+    ps.acc_light = at(B.light, B.light_layout);
+    ps.acc_light_grad = at(B.light_grad, B.light_grad_layout);
+}
+
+PTIR_DEV void add_material_output_grad(const TraceParams& P, const BwdInputs& B, unsigned x, unsigned y, unsigned z,
+                                       size_t li, Segment& s) {
+    if (!s.ivalid || !B.material_grad) return;
+    const SampleLayout& L = B.material_grad_layout;
+    const long long off = sample_offset(L, P.flat_samples != 0, z, y, x, li);
+    s.d_albedo += ld_sample3(B.material_grad, L, off);
+    s.d_rough += __ldg(B.material_grad + off + 3 * L.sc);
+    if (P.flags & kMetallic) s.d_metal += __ldg(B.material_grad + off + 4 * L.sc);
 }
 
 PTIR_DEV unsigned effective_bounces(const TraceParams& P) {
@@ -494,7 +555,7 @@ PTIR_DEV void composite_one(const TraceParams& P, TraceCounters& ctr, Composite&
         if (vis) vis[id] = __int_as_float(1);
     }
     c.last_hit = fmaxf(c.last_hit, t);
-    if (P.flags & kHitCounts) c.hits_count += accept ? 1.0f : 0.0f;
+    c.hits_count += accept ? 1.0f : 0.0f;  // the output is written only with kHitCounts
 }
 
 // Composite one k-buffer batch held in registers.

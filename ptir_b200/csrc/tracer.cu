@@ -28,10 +28,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_fwd(TraceParams P
         path_init(ps, effective_bounces(P));
         Segment s;
         float3 o, d;
-        world_ray(P, view, li, o, d);
+        world_ray(P, view, x, y, z, li, o, d);
         segment_reset(s, o, d, 0.0f);
         ++ctr.segments;
         intersect_mark<false>(C, s, rng, O.visibility);
+        sig_event(P, ps, sig_segment(s));
         // primary outputs (pathTracer.cuh:636-663)
         {
             float* r = O.radiance + 3 * li;
@@ -58,11 +59,15 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_fwd(TraceParams P
                 if (!ps.active) break;
                 ps.bounces = depth + 1u;
                 sample_next(C, ps, s, rng);
-                if (max3(ps.throughput) < 1e-4f) break;
+                const bool cont = path_continues(ps);
+                sig_event(P, ps, kSigCont | (cont ? 1u : 0u));
+                if (!cont) break;
                 ++ctr.segments;
                 intersect_mark<true>(C, s, rng, O.visibility);
+                sig_event(P, ps, sig_segment(s));
             }
         }
+        if (O.path_sig) O.path_sig[li] = ps.sig;
         // PBR outputs (pathTracer.cuh:665-681); zero when the primary ray found no surface
         float* pb = O.pbr + 3 * li;
         pb[0] = ps.acc.x; pb[1] = ps.acc.y; pb[2] = ps.acc.z;
@@ -90,22 +95,14 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_bwd(TraceParams P
         rng.seed(x, y, z, P.views[view].frame);
         PathState ps;
         path_init(ps, effective_bounces(P));
-        ps.acc = ld3(B.pbr + 3 * li);
-        ps.acc_grad = B.pbr_grad ? ld3(B.pbr_grad + 3 * li) : f3(0.0f);
-        ps.acc_light = ld3(B.light + 3 * li);
-        ps.acc_light_grad = B.light_grad ? ld3(B.light_grad + 3 * li) : f3(0.0f);
+        load_adjoint_inputs(P, B, x, y, z, li, ps);
         Segment s;
         float3 o, d;
-        world_ray(P, view, li, o, d);
+        world_ray(P, view, x, y, z, li, o, d);
         segment_reset(s, o, d, 0.0f);
         ++ctr.segments;
         intersect_mark<false>(C, s, rng, nullptr);
-        if (s.ivalid && B.material_grad) {
-            const float* mg = B.material_grad + 5 * li;
-            s.d_albedo += ld3(mg);
-            s.d_rough += __ldg(mg + 3);
-            if (P.flags & kMetallic) s.d_metal += __ldg(mg + 4);
-        }
+        add_material_output_grad(P, B, x, y, z, li, s);
         if ((P.flags & kVisualizeLights) || s.ivalid) {
             if (P.flags & kMis) sample_nee(C, ps, s, rng);
             for (unsigned depth = 0; depth < ps.max_bounces && ps.active; ++depth) {

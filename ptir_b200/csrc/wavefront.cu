@@ -99,6 +99,7 @@ PTIR_DEV void write_pbr(const FwdOutputs& O, size_t li, const PathState& ps) {
     float* cp = O.components + 6 * li;
     cp[0] = ps.acc_direct.x; cp[1] = ps.acc_direct.y; cp[2] = ps.acc_direct.z;
     cp[3] = ps.acc_indirect.x; cp[4] = ps.acc_indirect.y; cp[5] = ps.acc_indirect.z;
+    if (O.path_sig) O.path_sig[li] = ps.sig;
 }
 
 #define PTIR_STAGE_PROLOGUE                         \
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_camera(TraceParams P, WfView
             rng.seed(x, y, z, P.views[view].frame);
             Segment s;
             float3 o, d;
-            world_ray(P, view, li, o, d);
+            world_ray(P, view, x, y, z, li, o, d);
             segment_reset(s, o, d, 0.0f);
             W.seg[q] = s;
             store_rng(W, q, rng);
@@ -372,6 +373,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_primary(TraceParams P, F
             PathState ps;
             path_init(ps, effective_bounces(P));
             Segment s = W.seg[q];
+            sig_event(P, ps, sig_segment(s));
             float* r = O.radiance + 3 * li;
             r[0] = s.radiance.x; r[1] = s.radiance.y; r[2] = s.radiance.z;
             O.density[li] = 1.0f - s.transmittance;
@@ -514,6 +516,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, 
                 emitter_clear(em);
                 W.ps[q].em = em;
             }
+            if (P.flags & kPathSig) W.ps[q].sig = sig_mix(W.ps[q].sig, kSigShadow | (occluded ? 1u : 0u));
             store_rng(W, q, rng);
             phase = kIdle;
         }
@@ -538,12 +541,14 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_bounce(TraceParams P, Fw
             Segment s = W.seg[q];
             PathState ps = W.ps[q];
             Pcg32 rng = load_rng(W, q);
+            if (depth > 0) sig_event(P, ps, sig_segment(s));
             accumulate_light(C, ps, s);
             ps.active &= (unsigned)((depth + 1u < ps.max_bounces) && s.ivalid);
             if (ps.active) {
                 ps.bounces = depth + 1u;
                 sample_next(C, ps, s, rng);
-                cont = ps.active && !(max3(ps.throughput) < 1e-4f);
+                cont = path_continues(ps);
+                sig_event(P, ps, kSigCont | (cont ? 1u : 0u));
             }
             if (cont) {
                 W.seg[q] = s;
@@ -583,17 +588,9 @@ __global__ void __launch_bounds__(kMaxThreads) k_wb_primary(TraceParams P, BwdIn
             Pcg32 rng = load_rng(W, q);
             PathState ps;
             path_init(ps, effective_bounces(P));
-            ps.acc = ld3(B.pbr + 3 * li);
-            ps.acc_grad = B.pbr_grad ? ld3(B.pbr_grad + 3 * li) : f3(0.0f);
-            ps.acc_light = ld3(B.light + 3 * li);
-            ps.acc_light_grad = B.light_grad ? ld3(B.light_grad + 3 * li) : f3(0.0f);
+            load_adjoint_inputs(P, B, x, y, z, li, ps);
             Segment s = W.seg[q];
-            if (s.ivalid && B.material_grad) {
-                const float* mg = B.material_grad + 5 * li;
-                s.d_albedo += ld3(mg);
-                s.d_rough += __ldg(mg + 3);
-                if (P.flags & kMetallic) s.d_metal += __ldg(mg + 4);
-            }
+            add_material_output_grad(P, B, x, y, z, li, s);
             cont = (P.flags & kVisualizeLights) || s.ivalid;
             if (cont) {
                 if (mis) shadow = nee_prepare(C, ps, s, rng);

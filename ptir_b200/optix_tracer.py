@@ -30,6 +30,24 @@ def _f32(t: torch.Tensor, name: str) -> torch.Tensor:
     return t.contiguous()
 
 
+def _f32_strided(t: torch.Tensor, name: str) -> torch.Tensor:
+    """A per-sample float32 CUDA tensor passed with its own strides, as the reference's
+    PackedTensorAccessor32 reads it (tensorBuffering.h:41-45): no copy, whatever its layout."""
+    if not isinstance(t, torch.Tensor):
+        raise TypeError(f"{name}: expected a torch.Tensor")
+    if t.dtype != torch.float32:
+        raise TypeError(f"{name}: unsupported dtype {t.dtype} (float32 required)")
+    if not t.is_cuda:
+        raise ValueError(f"{name}: CUDA tensor required")
+    return t
+
+
+def _strides4(t: torch.Tensor | None):
+    """The element strides of a [Z,H,W,C] (or [1,1,T,C]) tensor for a `*_strides[4]` field."""
+    s = (0, 0, 0, 0) if t is None else tuple(int(v) for v in t.stride())
+    return (C.c_int64 * 4)(*s)
+
+
 def _stream() -> int:
     return torch.cuda.current_stream().cuda_stream
 
@@ -171,7 +189,7 @@ class OptixTracer:
         t2w = _f32(ray_to_world, "ray_to_world")
         if t2w.numel() < 12:
             raise ValueError("ray_to_world must hold at least one 3x4 (or 4x4) transform")
-        ori, dirs = _f32(ray_ori, "ray_ori"), _f32(ray_dir, "ray_dir")
+        ori, dirs = _f32_strided(ray_ori, "ray_ori"), _f32_strided(ray_dir, "ray_dir")
         if ori.dim() != 4 or ori.shape[-1] != 3 or dirs.shape != ori.shape:
             raise ValueError("ray_ori / ray_dir must be [Z,H,W,3]")
         dens = _f32(particle_density, "particle_density")
@@ -201,6 +219,7 @@ class OptixTracer:
         a.frame = int(frame) & 0xFFFFFFFF
         a.ray_to_world = _ptr(t2w)
         a.ray_origin, a.ray_direction = _ptr(ori), _ptr(dirs)
+        a.ray_origin_strides, a.ray_direction_strides = _strides4(ori), _strides4(dirs)
         a.z, a.h, a.w = int(ori.shape[0]), int(ori.shape[1]), int(ori.shape[2])
         a.particle_density, a.particle_material, a.particle_radiance = _ptr(dens), _ptr(mat), _ptr(rad)
         a.particle_shading_normal = _ptr(snrm)
@@ -227,10 +246,12 @@ class OptixTracer:
     def trace(self, frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material, particle_radiance,
               particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
               mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table, sh_indirect,
-              sph_degree, min_transmittance, max_bounces, _views=None):
+              sph_degree, min_transmittance, max_bounces, _views=None, path_signature=None):
         """trace (optixTracer.cpp:909-1013). Returns (rayRad, rayDns, rayHit[...,2], rayHitSecondMoment,
         rayDepthDistortion, rayNrm, rayShadingNrm, rayMaterial, rayHitsCount, particleVisibility, rayPbr,
-        rayLight, rayPbrComponents)."""
+        rayLight, rayPbrComponents). `path_signature` (not in the reference): an int32 CUDA tensor of
+        Z*H*W elements, contiguous, filled with each path's decision signature (a hash of its
+        discrete branches, include/ptir_b200.h), for parity diagnostics."""
         a, keep, zhw, n, _ = self._args(frame, ray_to_world, ray_ori, ray_dir, particle_density, particle_material,
                                         particle_radiance, particle_shading_normal, environment, environment_alias_table,
                                         lights, light_alias_table, mesh_light_vertices, mesh_light_triangles,
@@ -243,10 +264,16 @@ class OptixTracer:
         vis = torch.empty((n, 1), dtype=torch.float32, device=dev)
         pbr, light = e(3), e(3)
         comps = torch.empty((*zhw, 2, 3), dtype=torch.float32, device=dev)
+        sig = None
+        if path_signature is not None:
+            sig = path_signature
+            if (sig.dtype != torch.int32 or not sig.is_cuda or not sig.is_contiguous()
+                    or sig.numel() != int(zhw[0]) * int(zhw[1]) * int(zhw[2])):
+                raise ValueError("path_signature must be a contiguous int32 CUDA tensor with one element per sample")
         o = N.PtirTraceOutputs(
             _ptr(out["radiance"]), _ptr(out["density"]), _ptr(out["hit"]), _ptr(out["hit2"]), _ptr(out["distortion"]),
             _ptr(out["normal"]), _ptr(out["snormal"]), _ptr(out["material"]), _ptr(out["hits"]), _ptr(pbr),
-            _ptr(light), _ptr(comps), _ptr(vis))
+            _ptr(light), _ptr(comps), _ptr(vis), _ptr(sig))
         if _views is None:
             rc = self._lib.ptir_trace(self._h, C.byref(a), C.byref(o), _stream())
         else:
@@ -276,8 +303,8 @@ class OptixTracer:
         def g(t, c, name):
             if t is None:
                 return None
-            t = _f32(t, name)
-            if tuple(t.shape[:3]) != tuple(zhw) or t.shape[-1] != c:
+            t = _f32_strided(t, name)
+            if t.dim() != 4 or tuple(t.shape[:3]) != tuple(zhw) or t.shape[-1] != c:
                 raise ValueError(f"{name} must be [Z,H,W,{c}]")
             return t
 
@@ -291,7 +318,8 @@ class OptixTracer:
         snrm_grad = (torch.zeros_like(particle_shading_normal) if particle_shading_normal is not None
                      else torch.zeros((n, 3), dtype=torch.float32, device=dev))
         env_grad = torch.zeros_like(environment)
-        b = N.PtirBwdArgs(_ptr(pbr), _ptr(light), _ptr(pbr_g), _ptr(light_g), _ptr(mat_g))
+        b = N.PtirBwdArgs(_ptr(pbr), _ptr(light), _ptr(pbr_g), _ptr(light_g), _ptr(mat_g), _strides4(pbr),
+                          _strides4(light), _strides4(pbr_g), _strides4(light_g), _strides4(mat_g))
         o = N.PtirBwdOutputs(_ptr(material_grad), _ptr(env_grad) if env is not None else None)
         if _views is None:
             rc = self._lib.ptir_trace_bwd(self._h, C.byref(a), C.byref(b), C.byref(o), _stream())
@@ -323,20 +351,22 @@ class OptixTracer:
     def trace_views(self, views, ray_ori, ray_dir, particle_density, particle_material, particle_radiance,
                     particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
                     mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table,
-                    sh_indirect, sph_degree, min_transmittance, max_bounces):
+                    sh_indirect, sph_degree, min_transmittance, max_bounces, path_signature=None):
         """trace() over a batch of views of their own extent and sample count, in one launch
         sequence. `views` lists (frame, ray_to_world, z, h, w); ray_ori / ray_dir are the views'
         [Z,H,W,3] rays concatenated in view order, [T,3]. Returns the 13 outputs of trace() with
         every per-sample output flat, [T,C] (split_views() cuts them per view); each view's
         values are those of its own trace() call."""
         table, keep_t, total = self._view_table(views)
-        ori, dirs = _f32(ray_ori, "ray_ori").reshape(1, 1, -1, 3), _f32(ray_dir, "ray_dir").reshape(1, 1, -1, 3)
+        ori = _f32_strided(ray_ori, "ray_ori").reshape(1, 1, -1, 3)
+        dirs = _f32_strided(ray_dir, "ray_dir").reshape(1, 1, -1, 3)
         if ori.shape[2] != total or dirs.shape != ori.shape:
             raise ValueError(f"ray_ori / ray_dir must hold the {total} rays of the views")
         out = self.trace(views[0][0], keep_t[0], ori, dirs, particle_density, particle_material, particle_radiance,
                          particle_shading_normal, environment, environment_alias_table, lights, light_alias_table,
                          mesh_light_vertices, mesh_light_triangles, mesh_lights, mesh_light_triangle_alias_table,
-                         sh_indirect, sph_degree, min_transmittance, max_bounces, _views=table)
+                         sh_indirect, sph_degree, min_transmittance, max_bounces, _views=table,
+                         path_signature=path_signature)
         flat = [t if k == 9 else t.reshape(total, *t.shape[3:]) for k, t in enumerate(out)]
         del keep_t
         return tuple(flat)
@@ -352,7 +382,7 @@ class OptixTracer:
         """trace_bwd() over a batch of views; per-sample inputs flat [T,C] as trace_views() returns them."""
         table, keep_t, total = self._view_table(views)
         r = lambda t: None if t is None else t.reshape(1, 1, total, -1)  # noqa: E731
-        ori, dirs = r(_f32(ray_ori, "ray_ori")), r(_f32(ray_dir, "ray_dir"))
+        ori, dirs = r(_f32_strided(ray_ori, "ray_ori")), r(_f32_strided(ray_dir, "ray_dir"))
         res = self.trace_bwd(views[0][0], keep_t[0], ori, dirs, r(ray_rad), r(ray_dns), r(ray_hit),
                              r(ray_hit_second_moment), r(ray_depth_distortion), r(ray_nrm), r(ray_shading_nrm),
                              r(ray_material), r(ray_pbr), r(ray_light), particle_density, particle_material,
