@@ -96,16 +96,20 @@ class Setup:
         env = synthetic.make_environment(*wl.env_hw, seed=wl.seed)
         self.env = d(env)
         self.alias = envmap.pack(envmap.build(env), device)
-        # with W ranks the job has W x views views and this rank traces its shard
+        # With W ranks the job has W x views views; this rank traces its share, balanced by the
+        # views' samples (the estimate of their path segments).
         world = int(os.environ.get("WORLD_SIZE", "1"))
-        all_eyes = synthetic.camera_positions(len(wl.views) * world, seed=wl.seed)
-        eyes = all_eyes[list(pdist.shard(len(all_eyes), rank, world))]
+        job_views = list(wl.views) * world
+        all_eyes = synthetic.camera_positions(len(job_views), seed=wl.seed)
+        mine = pdist.shard_weighted([w * h * spp for w, h, spp in job_views], rank, world)
+        eyes = all_eyes[mine]
+        self.my_views = [job_views[i] for i in mine]
         self.t2w = torch.eye(4, device=device).reshape(1, 4, 4).contiguous()
-        self.batched = any(v != wl.views[0] for v in wl.views)
+        self.batched = any(v != self.my_views[0] for v in self.my_views)
         oris, dirs = [], []
         if not self.batched:
             # one launch: z = sample * views + view (the reference's order)
-            w, h, spp = wl.views[0]
+            w, h, spp = self.my_views[0]
             for eye in eyes:
                 o, dr = synthetic.view_rays_device(w, h, spp, eye, device)
                 oris.append(o)
@@ -115,7 +119,7 @@ class Setup:
         else:
             # views of their own resolution and spp, one batch: rays flat in view order
             self.views = []
-            for v, ((w, h, spp), eye) in enumerate(zip(wl.views, eyes)):
+            for v, ((w, h, spp), eye) in enumerate(zip(self.my_views, eyes)):
                 o, dr = synthetic.view_rays_device(w, h, spp, eye, device)
                 oris.append(o.reshape(-1, 3))
                 dirs.append(dr.reshape(-1, 3))
@@ -373,6 +377,8 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, schedule="megakernel")
     if args.chunk_tiles:
         shape = dict(shape, chunk_tiles=args.chunk_tiles)
+    if args.exact_candidates:
+        shape = dict(shape, exact_candidates=True)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     backward = S.wl.backward
@@ -388,6 +394,7 @@ def run_ours(args, rank, world, device):
     material = S.material.clone().requires_grad_(backward)
     env = S.env.clone().requires_grad_(backward)
     adam = {k: (torch.zeros_like(t), torch.zeros_like(t)) for k, t in (("material", material), ("env", env))}
+    bucket = pdist.GradientBucket()  # the all-reduce's flat buffer, allocated once
     # the step's ray inputs (device buffers, refilled from pinned host memory every timed step)
     ori_d, dir_d = S.ray_ori.clone(), S.ray_dir.clone()
     use_autograd = backward and not S.batched and not args.graph
@@ -444,7 +451,7 @@ def run_ours(args, rank, world, device):
         if on_bwd:
             on_bwd()
         if world > 1:
-            pdist.allreduce_gradients([mg, eg])
+            bucket.allreduce([mg, eg])
         with torch.no_grad():
             selective_adam_(material, mg, *adam["material"], vis.view(torch.int32) != 0, lr=ADAM_LR)
             selective_adam_(env, eg, *adam["env"], None, lr=ADAM_LR)
@@ -780,6 +787,8 @@ def main():
                     help="one gradient atomic per lane and term (default: warp-aggregated rows)")
     ap.add_argument("--kbuffer", type=int, default=0, choices=(0, 8, 16, 24, 32),
                     help="candidates per traversal (0: the tuned or default size)")
+    ap.add_argument("--exact-candidates", action="store_true",
+                    help="every traversal returns exactly the K nearest candidates (order independent)")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

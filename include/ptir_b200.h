@@ -101,6 +101,14 @@ typedef struct ptir_config {
                                      (default), 1 = one atomic per lane and term as the reference */
     int32_t shadow_kbuffer;       /* wavefront: candidates per NEE shadow-ray traversal, 8, 16 or 32 (0 = 16);
                                      a shadow walk visits hits in distance order whatever the size */
+    int32_t exact_candidates;     /* 0 = subtrees culled at the K-th distance by their box entry, as the
+                                     reference's traversal culls: a Gaussian whose closest approach lies
+                                     before its box entry (a ray grazing a box corner) is kept or not
+                                     depending on the traversal order; 1 = every traversal returns exactly
+                                     the K nearest candidates (its subtrees culled only when no closest
+                                     approach under them can lie before the K-th distance), so the results
+                                     depend on neither the order nor the k-buffer size (no counterpart in
+                                     the reference) */
 } ptir_config;
 
 enum { PTIR_STORAGE_FP32 = 0, PTIR_STORAGE_BF16 = 1, PTIR_STORAGE_FP16 = 2 };
@@ -311,18 +319,22 @@ const char* ptir_last_error(const ptir_tracer* tracer);
  * reserves all device memory for its own pool at start-up, or a plugin whose host forbids
  * device allocation after initialisation. For them a cudaMalloc fails or stalls the device.
  * It writes the scene AABB of the Gaussians' instance boxes (the bounds every trace clips
- * its rays to, identical to ptir_scene_bounds after ptir_build_bvh) into bounds_out:
- * 8 floats, lo.xyz 0 hi.xyz 0, device memory, 16-byte aligned. Inputs are device pointers as in
- * ptir_build_bvh, and kernel_degree / kernel_min_response / density_clamping are the
- * ptir_config fields. No handle is needed and nothing is allocated: the only scratch is a
- * fixed 128 KiB device array in the library.
- * Limit: N <= 8,388,608; larger N returns PTIR_EINVAL. The first call on a device resolves the
- * array's device address, so make that first call before any stream capture. Calls share the
- * array: calls that overlap on the GPU (unordered streams) race. Errors are also described in
- * err[err_len] when err is not NULL. */
+ * its rays to, identical to ptir_scene_bounds after ptir_build_bvh of a tracer with the same
+ * options) into bounds_out: 8 floats, lo.xyz 0 hi.xyz 0, device memory, 16-byte aligned. Inputs
+ * are device pointers as in ptir_build_bvh; kernel_degree / kernel_min_response /
+ * density_clamping / storage are the ptir_config fields (with BF16 / FP16 storage the
+ * attributes are rounded as ptir_build_bvh rounds them). No handle is needed and nothing is
+ * allocated: the only scratch is a fixed 128 KiB device array in the library.
+ * Limit: N <= 8,388,608; larger N returns PTIR_EINVAL. N = 0 writes the empty box, lo = +3e38
+ * and hi = -3e38 on every axis (ptir_scene_bounds has no structure to read then and returns
+ * PTIR_ESTATE). The first call on a device resolves the array's device address, so make that
+ * first call before any stream capture; the address is kept, so do not use the library across a
+ * cudaDeviceReset. Calls share the array: calls that overlap on the GPU (unordered streams)
+ * race. Errors are also described in err[err_len] when err is not NULL. */
 int ptir_instance_bounds_noalloc(float kernel_degree, float kernel_min_response, int32_t density_clamping,
-                                 const float* pos, const float* rot, const float* scl, const float* dns, int32_t n,
-                                 float* bounds_out, void* stream, char* err, int32_t err_len);
+                                 int32_t storage, const float* pos, const float* rot, const float* scl,
+                                 const float* dns, int32_t n, float* bounds_out, void* stream, char* err,
+                                 int32_t err_len);
 
 #ifdef __cplusplus
 }

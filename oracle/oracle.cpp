@@ -7,6 +7,7 @@
 #include <array>
 #include <initializer_list>
 #include <limits>
+#include <string>
 #include <utility>
 
 namespace oracle {
@@ -255,6 +256,11 @@ public:
             tx = std::fmin(tx, t1);
         }
         if (te > tx) return false;
+        return instance_hit(o, d, tmin, tend, tstar);
+    }
+
+    // intersectInstanceParticle (gaussianParticles.cuh:484-500), object-space ray (o, d)
+    static bool instance_hit(const V3<T>& o, const V3<T>& d, T tmin, T tend, T& tstar) {
         const T dd = dot(d, d);
         const T den = T(1) / dd;
         tstar = -dot(o, d) * den;
@@ -372,6 +378,40 @@ public:
         return {std::fmax(rad.x, T(0)), std::fmax(rad.y, T(0)), std::fmax(rad.z, T(0))};
     }
 
+    // The compositing state of processHit (gaussianParticles.cuh:343-440): transmittance, radiance,
+    // depth and its second moment, material and shading normal sums, normal.
+    struct HitSums {
+        T transmittance = 1, depth = 0, depth2 = 0, rgh = 0, met = 0;
+        V3<T> radiance{}, alb{}, snrm{}, normal{};
+    };
+
+    // gaussianParticles.cuh:343-440: response of Gaussian `id` to the ray; when accepted, its
+    // weighted contributions are added to the sums and the transmittance falls. Returns accepted.
+    bool process_hit(uint32_t id, const Ray<T>& ray, HitSums& h) const {
+        const Density D = fetch_density(id);
+        V3<T> gro, grd; T d2, gres, ga;
+        response(D, ray, gro, grd, d2, gres, ga);
+        if (!(gres > min_resp && ga > alpha_min)) return false;
+        const T wgt = ga * h.transmittance;
+        const V3<T> grds = D.scl * grd * dot(grd, -gro);
+        const T hit_t = std::sqrt(dot(grds, grds));
+        h.radiance += sh_radiance(id, ray.d) * wgt;
+        const float* m = in.material + 5 * size_t(id);
+        h.alb += v3<T>(m[0], m[1], m[2]) * wgt;
+        h.rgh += T(m[3]) * wgt;
+        h.met += T(m[4]) * wgt;
+        h.transmittance *= (T(1) - ga);
+        h.depth += hit_t * wgt;
+        h.depth2 += hit_t * hit_t * wgt;
+        if (cfg.enable_normals) {
+            const float* n = in.snrm + 3 * size_t(id);
+            h.snrm += v3<T>(n[0], n[1], n[2]) * wgt;
+            const V3<T> srot = colmul(D.rt, D.scl);
+            h.normal += safe_normalize((gro + grd * (dot(grd, -gro) - std::sqrt(T(9) - d2))) * srot) * wgt;
+        }
+        return true;
+    }
+
     // pathTracer.cuh:216-311 (+ processHit, gaussianParticles.cuh:343-440)
     void ray_intersect(bool self_occ, const Ray<T>& ray, RayPayload<T>& p, Sampler& s) {
         T t0, t1;
@@ -379,61 +419,43 @@ public:
         const T spdf = p.scatter_pdf, lpdf = p.light_pdf;
         p = RayPayload<T>(ray, std::fmax(T(0), float_offset(t0, -1e-9f)));
         if (cfg.enable_mis) { p.scatter_pdf = spdf; p.light_pdf = lpdf; }
-        T depth = 0;
-        V3<T> m_alb{}, snrm{};
-        T m_rgh = 0, m_met = 0;
+        HitSums sums;
         std::array<Hit, kK> hits;
-        while (p.last_hit <= t1 && p.transmittance > T(in.min_transmittance)) {
+        while (p.last_hit <= t1 && sums.transmittance > T(in.min_transmittance)) {
             trace(hits, p.ray, float_offset(p.last_hit, 1e-9f), float_offset(t1, 1e-9f));
             if (hits[0].id == kInvalid) break;
             for (int i = 0; i < kK; ++i) {
                 const Hit& h = hits[i];
-                if (h.id == kInvalid || !(p.transmittance > T(in.min_transmittance))) continue;
+                if (h.id == kInvalid || !(sums.transmittance > T(in.min_transmittance))) continue;
                 if (self_occ && self_occlusion(h, p.ray)) { p.last_hit = std::fmax(p.last_hit, T(h.t)); continue; }
-                const Density D = fetch_density(h.id);
-                V3<T> gro, grd; T d2, gres, ga;
-                response(D, p.ray, gro, grd, d2, gres, ga);
-                const bool accept = gres > min_resp && ga > alpha_min;
+                const bool accept = process_hit(h.id, p.ray, sums);
                 if (accept) {
                     st.accepted++;
-                    const T wgt = ga * p.transmittance;
-                    const V3<T> grds = D.scl * grd * dot(grd, -gro);
-                    const T hit_t = std::sqrt(dot(grds, grds));
-                    p.radiance += sh_radiance(h.id, p.ray.d) * wgt;
-                    const float* m = in.material + 5 * size_t(h.id);
-                    m_alb += v3<T>(m[0], m[1], m[2]) * wgt;
-                    m_rgh += T(m[3]) * wgt;
-                    m_met += T(m[4]) * wgt;
-                    p.transmittance *= (T(1) - ga);
-                    depth += hit_t * wgt;
-                    p.hit2 += hit_t * hit_t * wgt;
-                    if (cfg.enable_normals) {
-                        const float* n = in.snrm + 3 * size_t(h.id);
-                        snrm += v3<T>(n[0], n[1], n[2]) * wgt;
-                        const V3<T> srot = colmul(D.rt, D.scl);
-                        p.normal += safe_normalize((gro + grd * (dot(grd, -gro) - std::sqrt(T(9) - d2))) * srot) * wgt;
-                    }
                     p.hit = 1;
-                    const T op = T(1) - p.transmittance;
-                    p.distortion = std::fmax(op * p.hit2 - depth * depth, T(0));
+                    const T op = T(1) - sums.transmittance;
+                    p.distortion = std::fmax(op * sums.depth2 - sums.depth * sums.depth, T(0));
                     if (visibility) visibility[h.id] = 1.0f;
                 }
                 p.last_hit = std::fmax(p.last_hit, T(h.t));
                 p.hits_count += accept ? T(1) : T(0);  // output only with enable_hitcounts
             }
         }
+        p.transmittance = sums.transmittance;
+        p.radiance = sums.radiance;
+        p.hit2 = sums.depth2;
+        p.normal = sums.normal;
         const T op = T(1) - p.transmittance;
-        p.hit_distance = depth;
+        p.hit_distance = sums.depth;
         p.valid = false;
         if (p.hit && op > T(0.5)) {
             const T inv = T(1) / std::fmax(op, T(1e-12));
-            const T dd = depth * inv;
+            const T dd = sums.depth * inv;
             p.inter.valid = true;
             p.inter.position = p.ray.o + p.ray.d * dd;
-            p.inter.snormal = snrm * inv;
-            p.inter.albedo = m_alb * inv;
-            p.inter.roughness = m_rgh * inv;
-            p.inter.metallic = m_met * inv;
+            p.inter.snormal = sums.snrm * inv;
+            p.inter.albedo = sums.alb * inv;
+            p.inter.roughness = sums.rgh * inv;
+            p.inter.metallic = sums.met * inv;
         } else {
             const T u = s.next_1d();
             p.valid = u < p.transmittance;
@@ -1691,16 +1713,17 @@ static int run_bwd(const orc_config* c, const orc_scene* s, const orc_bwd_in* b,
 
 extern "C" {
 
-int orc_trace_f64(const orc_config* c, const orc_scene* s, const orc_fwd_out* o, int nthreads, orc_stats* stats) {
-    return run_fwd<double>(c, s, o, nthreads, 1, stats);
+int orc_trace_f64(const orc_config* c, const orc_scene* s, const orc_fwd_out* o, int nthreads, long long stride,
+                  orc_stats* stats) {
+    return run_fwd<double>(c, s, o, nthreads, stride, stats);
 }
 int orc_trace_f32(const orc_config* c, const orc_scene* s, const orc_fwd_out* o, int nthreads, long long stride,
                   orc_stats* stats) {
     return run_fwd<float>(c, s, o, nthreads, stride, stats);
 }
 int orc_trace_bwd_f64(const orc_config* c, const orc_scene* s, const orc_bwd_in* b, double* mat_grad, double* env_grad,
-                      int nthreads, orc_stats* stats) {
-    return run_bwd<double>(c, s, b, mat_grad, env_grad, nthreads, 1, stats);
+                      int nthreads, long long stride, orc_stats* stats) {
+    return run_bwd<double>(c, s, b, mat_grad, env_grad, nthreads, stride, stats);
 }
 int orc_trace_bwd_f32(const orc_config* c, const orc_scene* s, const orc_bwd_in* b, double* mat_grad, double* env_grad,
                       int nthreads, long long stride, orc_stats* stats) {
@@ -1758,6 +1781,90 @@ int orc_num_threads(void) { return omp_get_max_threads(); }
 // Light samples from positions pos [m,3], sample i drawn from the launch stream (i, 0, 0, frame):
 // out [m,9] = wi xyz, Li rgb, pdf, dist, type; eval_pdf [m] = the light sampler's pdf of the
 // sampled direction (lightSampler.cuh:340-406). FP64.
+// Known-answer evaluations of single reference functions, the cases of tests/golden/device_kat.npz
+// (inputs and outputs laid out as the reference kernels of oracle/ref_device_kat.cu lay them out),
+// in FP64. env_grad [eh, ew, 4] receives the environment gradient of "env_bwd".
+int orc_kat(const orc_config* c, const orc_scene* sc, const char* name, int n, const float* in, double* out,
+            double* env_grad) {
+    const Config cfg = to_cfg(c);
+    const Inputs inp = to_in(sc);
+    Instances<double> I;
+    build_instances<double>(cfg, inp, I);
+    Tracer<double> tr(cfg, inp, I);
+    std::vector<double> eg(size_t(std::max(inp.eh, 0)) * std::max(inp.ew, 0) * 4, 0.0);
+    tr.env_grad = &eg;
+    using V = V3<double>;
+    const std::string what(name);
+    auto v3f = [](const float* p) { return V{double(p[0]), double(p[1]), double(p[2])}; };
+    auto put3 = [](double* o, const V& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; };
+    for (int i = 0; i < n; ++i) {
+        if (what == "process_hit") {
+            const float* a = in + 8 * size_t(i);
+            Tracer<double>::HitSums h;
+            h.transmittance = a[7];
+            const bool acc = tr.process_hit(uint32_t(a[6]), Ray<double>{v3f(a), v3f(a + 3)}, h);
+            double* o = out + 18 * size_t(i);
+            o[0] = acc ? 1.0 : 0.0; o[1] = h.transmittance; put3(o + 2, h.radiance); o[5] = h.depth; o[6] = h.depth2;
+            put3(o + 7, h.alb); o[10] = h.rgh; o[11] = h.met; put3(o + 12, h.snrm); put3(o + 15, h.normal);
+        } else if (what == "intersect") {
+            const float* a = in + 8 * size_t(i);
+            double t = 0.0;
+            const bool hit = Tracer<double>::instance_hit(v3f(a), v3f(a + 3), a[6], a[7], t);
+            out[2 * size_t(i)] = hit ? 1.0 : 0.0;
+            out[2 * size_t(i) + 1] = t;
+        } else if (what == "brdf_sample" || what == "brdf_eval" || what == "brdf_grads") {
+            const float* a = in + 16 * size_t(i);
+            const V wo = v3f(a), nrm = v3f(a + 3), alb = v3f(a + 6), r3 = v3f(a + 11);
+            double pdf = 0.0;
+            if (what == "brdf_eval") {
+                put3(out + 4 * size_t(i), tr.eval_brdf(wo, nrm, alb, a[9], a[10], r3, pdf));
+                out[4 * size_t(i) + 3] = pdf;
+            } else if (what == "brdf_sample") {
+                V next{};
+                const V v = tr.sample_brdf(wo, nrm, alb, a[9], a[10], r3, next, pdf);
+                double* o = out + 7 * size_t(i);
+                put3(o, v); put3(o + 3, next); o[6] = pdf;
+            } else {
+                V next{};
+                const BrdfGrad<double> g = tr.sample_brdf_grad(wo, nrm, alb, a[9], a[10], r3, next, pdf);
+                double* o = out + 19 * size_t(i);
+                put3(o, g.value); put3(o + 3, g.d_albedo); put3(o + 6, g.d_metallic); put3(o + 9, g.d_roughness);
+                put3(o + 12, g.d_next_dir); put3(o + 15, next); o[18] = pdf;
+            }
+        } else if (what == "env_lookup") {
+            const V d = v3f(in + 3 * size_t(i));
+            put3(out + 4 * size_t(i), tr.background(d));
+            out[4 * size_t(i) + 3] = inp.ah > 0 ? tr.alias_pdf(d) : 0.0;
+        } else if (what == "env_bwd") {
+            const float* a = in + 6 * size_t(i);
+            V dir_grad{};
+            put3(out + 6 * size_t(i), tr.background_bwd(v3f(a), v3f(a + 3), &dir_grad));
+            put3(out + 6 * size_t(i) + 3, dir_grad);
+        } else if (what == "env_sample") {
+            const float* a = in + 4 * size_t(i);
+            Sampler s;
+            s.init_launch(unsigned(a[0]), unsigned(a[1]), unsigned(a[2]), unsigned(a[3]));
+            double pdf = 0.0;
+            put3(out + 4 * size_t(i), tr.sample_alias_dir(s, pdf));
+            out[4 * size_t(i) + 3] = pdf;
+        } else if (what == "light_sample") {
+            const float* a = in + 7 * size_t(i);
+            Sampler s;
+            s.init_launch(unsigned(a[3]), unsigned(a[4]), unsigned(a[5]), unsigned(a[6]));
+            const auto ls = tr.sample_light(v3f(a), s);
+            double* o = out + 9 * size_t(i);
+            put3(o, ls.wi); put3(o + 3, ls.Li); o[6] = ls.pdf; o[7] = ls.dist; o[8] = double(ls.type);
+        } else if (what == "light_pdf") {
+            const float* a = in + 6 * size_t(i);
+            out[i] = tr.light_pdf(v3f(a), v3f(a + 3));
+        } else {
+            return 1;
+        }
+    }
+    if (env_grad) std::copy(eg.begin(), eg.end(), env_grad);
+    return 0;
+}
+
 int orc_light_samples(const orc_config* c, const orc_scene* sc, int m, const float* pos, double* out,
                       double* eval_pdf) {
     const Config cfg = to_cfg(c);

@@ -78,11 +78,13 @@ class Stats(C.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}
 
 
-def build() -> str:
-    """Compile liboracle.so (and, when the reference checkout is present, oracle/_ref)."""
+def build(reference_root: str | None = None) -> str:
+    """Compile liboracle.so and libptir_kat.so, and with a reference checkout (the argument, else
+    $PTIR_REFERENCE_ROOT) the binaries of oracle/_ref compiled from its sources."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    if os.path.isdir("/root/reference/threedgptir_tracer"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    ref = reference_root or os.environ.get("PTIR_REFERENCE_ROOT")
+    if ref and os.path.isdir(os.path.join(ref, "threedgptir_tracer")):
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={os.path.abspath(ref)}"], check=True)
     return os.path.join(_HERE, "liboracle.so")
 
 
@@ -94,9 +96,10 @@ def lib():
             build()
         L = C.CDLL(path)
         P = C.POINTER
-        L.orc_trace_f64.argtypes = [P(_Config), P(_Scene), P(_FwdOut), C.c_int, P(Stats)]
+        L.orc_trace_f64.argtypes = [P(_Config), P(_Scene), P(_FwdOut), C.c_int, C.c_longlong, P(Stats)]
         L.orc_trace_f32.argtypes = [P(_Config), P(_Scene), P(_FwdOut), C.c_int, C.c_longlong, P(Stats)]
-        L.orc_trace_bwd_f64.argtypes = [P(_Config), P(_Scene), P(_BwdIn), P(C.c_double), P(C.c_double), C.c_int, P(Stats)]
+        L.orc_trace_bwd_f64.argtypes = [P(_Config), P(_Scene), P(_BwdIn), P(C.c_double), P(C.c_double), C.c_int,
+                                        C.c_longlong, P(Stats)]
         L.orc_trace_bwd_f32.argtypes = [P(_Config), P(_Scene), P(_BwdIn), P(C.c_double), P(C.c_double), C.c_int,
                                         C.c_longlong, P(Stats)]
         L.orc_trace_candidates.argtypes = [P(_Config), P(_Scene), C.c_int, _FP, _FP, _FP, P(C.c_uint), P(C.c_double)]
@@ -106,6 +109,7 @@ def lib():
         L.orc_launch_seed.restype = C.c_ulonglong
         L.orc_num_threads.restype = C.c_int
         L.orc_light_samples.argtypes = [P(_Config), P(_Scene), C.c_int, _FP, P(C.c_double), P(C.c_double)]
+        L.orc_kat.argtypes = [P(_Config), P(_Scene), C.c_char_p, C.c_int, _FP, P(C.c_double), P(C.c_double)]
         _LIB = L
     return _LIB
 
@@ -217,7 +221,8 @@ _FWD_CH = {"radiance": 3, "density": 1, "hit": 2, "hit2": 1, "distortion": 1, "n
 
 
 def trace(cfg: OracleConfig, scene: dict, precision: str = "f64", threads: int = 0, stride: int = 1):
-    """Forward trace. Returns (dict of outputs [nz,h,w,C] float32, visibility [n], Stats); the
+    """Forward trace of every `stride`-th path (flat launch index li % stride == 0; the others'
+    outputs stay zero). Returns (dict of outputs [nz,h,w,C] float32, visibility [n], Stats); the
     dict also holds 'path_sig' [nz,h,w] uint32, each path's decision signature (the hash the GPU
     tracer writes to its path_signature output)."""
     keep = _Keep()
@@ -231,8 +236,7 @@ def trace(cfg: OracleConfig, scene: dict, precision: str = "f64", threads: int =
     st = Stats()
     c = cfg._c()
     if precision == "f64":
-        assert stride == 1
-        rc = lib().orc_trace_f64(C.byref(c), C.byref(sc), C.byref(fo), threads, C.byref(st))
+        rc = lib().orc_trace_f64(C.byref(c), C.byref(sc), C.byref(fo), threads, stride, C.byref(st))
     else:
         rc = lib().orc_trace_f32(C.byref(c), C.byref(sc), C.byref(fo), threads, stride, C.byref(st))
     assert rc == 0
@@ -242,8 +246,9 @@ def trace(cfg: OracleConfig, scene: dict, precision: str = "f64", threads: int =
 
 def trace_bwd(cfg: OracleConfig, scene: dict, fwd: dict, grads: dict, precision: str = "f64", threads: int = 0,
               stride: int = 1):
-    """Backward (path replay). ``fwd`` holds 'pbr' and 'light'; ``grads`` holds 'pbr', 'light',
-    'material' output gradients. Returns (material_grad [n,5] f64, env_grad [eh,ew,4] f64, Stats)."""
+    """Backward (path replay) of every `stride`-th path. ``fwd`` holds 'pbr' and 'light'; ``grads``
+    holds 'pbr', 'light', 'material' output gradients. Returns (material_grad [n,5] f64, env_grad
+    [eh,ew,4] f64, Stats)."""
     keep = _Keep()
     sc = _scene(keep, scene)
     bi = _BwdIn(_f(keep.f32(fwd["pbr"])), _f(keep.f32(fwd["light"])), _f(keep.f32(grads.get("pbr"))),
@@ -254,9 +259,8 @@ def trace_bwd(cfg: OracleConfig, scene: dict, fwd: dict, grads: dict, precision:
     c = cfg._c()
     P = C.POINTER(C.c_double)
     if precision == "f64":
-        assert stride == 1
         rc = lib().orc_trace_bwd_f64(C.byref(c), C.byref(sc), C.byref(bi), mg.ctypes.data_as(P), eg.ctypes.data_as(P),
-                                     threads, C.byref(st))
+                                     threads, stride, C.byref(st))
     else:
         rc = lib().orc_trace_bwd_f32(C.byref(c), C.byref(sc), C.byref(bi), mg.ctypes.data_as(P), eg.ctypes.data_as(P),
                                      threads, stride, C.byref(st))
@@ -321,6 +325,30 @@ def light_samples(cfg: OracleConfig, scene: dict, positions: np.ndarray, frame: 
     rc = lib().orc_light_samples(C.byref(c), C.byref(sc), m, _f(pos), out.ctypes.data_as(P), ev.ctypes.data_as(P))
     assert rc == 0
     return out[:, :3], out[:, 3:6], out[:, 6], out[:, 7], out[:, 8].astype(np.int64), ev
+
+
+KAT_COLUMNS = {"process_hit": 18, "intersect": 2, "brdf_sample": 7, "brdf_eval": 4, "brdf_grads": 19,
+               "env_lookup": 4, "env_bwd": 6, "env_sample": 4, "light_sample": 9, "light_pdf": 1}
+
+
+def kat(cfg: OracleConfig, scene: dict, name: str, inputs: np.ndarray):
+    """The oracle's FP64 evaluation of one reference function on known-answer inputs laid out as
+    oracle/ref_device_kat.cu lays them out. Returns (outputs [n, KAT_COLUMNS[name]] f64,
+    environment gradient [eh, ew, 4] f64 of "env_bwd")."""
+    keep = _Keep()
+    s = dict(scene)
+    s.setdefault("ray_ori", np.zeros((1, 1, 1, 3), np.float32))
+    s.setdefault("ray_dir", np.zeros((1, 1, 1, 3), np.float32))
+    sc = _scene(keep, s)
+    x = keep.f32(inputs)
+    n = x.shape[0]
+    out = np.zeros((n, KAT_COLUMNS[name]), np.float64)
+    eg = np.zeros((max(sc.eh, 1), max(sc.ew, 1), 4), np.float64)
+    P = C.POINTER(C.c_double)
+    rc = lib().orc_kat(C.byref(cfg._c()), C.byref(sc), name.encode(), n, _f(x), out.ctypes.data_as(P),
+                       eg.ctypes.data_as(P))
+    assert rc == 0, name
+    return out, eg[: sc.eh, : sc.ew]
 
 
 def num_threads() -> int:

@@ -45,6 +45,7 @@ class PtirConfig(C.Structure):
         ("storage", C.c_int32),
         ("grad_aggregate", C.c_int32),
         ("shadow_kbuffer", C.c_int32),
+        ("exact_candidates", C.c_int32),
     ]
 
 

@@ -269,36 +269,38 @@ __global__ void k_even_depth(int n, const int* __restrict__ parent, unsigned* __
 }
 
 // 4-wide node of binary node b (even depth): the boxes of its children, a leaf child taken as
-// is, an internal child replaced by its own two children
+// is, an internal child replaced by its own two children; with each child the largest kernel
+// support radius (kmax) under it
 __global__ void k_emit4(int n, const float4* __restrict__ nodes, const unsigned* __restrict__ even,
                         const unsigned* __restrict__ slot4, float4* __restrict__ nodes4) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= n - 1 || !even[b]) return;
-    float lx[4], ly[4], lz[4], hx[4], hy[4], hz[4];
+    float lx[4], ly[4], lz[4], hx[4], hy[4], hz[4], km[4];
     int ch[4];
     int cnt = 0;
-    auto add = [&](int c, float3 lo, float3 hi) {
+    auto add = [&](int c, float3 lo, float3 hi, float k) {
         lx[cnt] = lo.x; ly[cnt] = lo.y; lz[cnt] = lo.z;
         hx[cnt] = hi.x; hy[cnt] = hi.y; hz[cnt] = hi.z;
+        km[cnt] = k;
         ch[cnt] = c < 0 ? c : (int)slot4[c];
         ++cnt;
     };
-    auto expand = [&](int c, float3 lo, float3 hi) {
+    auto expand = [&](int c, float3 lo, float3 hi, float k) {
         if (c < 0) {
-            add(c, lo, hi);
+            add(c, lo, hi, k);
             return;
         }
         const float4* nc = nodes + 4 * (size_t)c;
         const float4 a = nc[0], q = nc[1], r = nc[2], e = nc[3];
-        add(__float_as_int(e.x), make_float3(a.x, a.y, a.z), make_float3(a.w, q.x, q.y));
-        add(__float_as_int(e.y), make_float3(q.z, q.w, r.x), make_float3(r.y, r.z, r.w));
+        add(__float_as_int(e.x), make_float3(a.x, a.y, a.z), make_float3(a.w, q.x, q.y), e.z);
+        add(__float_as_int(e.y), make_float3(q.z, q.w, r.x), make_float3(r.y, r.z, r.w), e.w);
     };
     const float4* nb = nodes + 4 * (size_t)b;
     const float4 a = nb[0], q = nb[1], r = nb[2], e = nb[3];
-    expand(__float_as_int(e.x), make_float3(a.x, a.y, a.z), make_float3(a.w, q.x, q.y));
-    expand(__float_as_int(e.y), make_float3(q.z, q.w, r.x), make_float3(r.y, r.z, r.w));
+    expand(__float_as_int(e.x), make_float3(a.x, a.y, a.z), make_float3(a.w, q.x, q.y), e.z);
+    expand(__float_as_int(e.y), make_float3(q.z, q.w, r.x), make_float3(r.y, r.z, r.w), e.w);
     for (int k = cnt; k < 4; ++k) {
-        lx[k] = ly[k] = lz[k] = hx[k] = hy[k] = hz[k] = 0.0f;
+        lx[k] = ly[k] = lz[k] = hx[k] = hy[k] = hz[k] = km[k] = 0.0f;
         ch[k] = kNoChild;
     }
     float4* out = nodes4 + 8 * (size_t)slot4[b];
@@ -309,7 +311,7 @@ __global__ void k_emit4(int n, const float4* __restrict__ nodes, const unsigned*
     out[4] = make_float4(hy[0], hy[1], hy[2], hy[3]);
     out[5] = make_float4(hz[0], hz[1], hz[2], hz[3]);
     out[6] = make_float4(__int_as_float(ch[0]), __int_as_float(ch[1]), __int_as_float(ch[2]), __int_as_float(ch[3]));
-    out[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    out[7] = make_float4(km[0], km[1], km[2], km[3]);
 }
 
 template <class T>
@@ -458,7 +460,10 @@ void accel_free(AccelState& st) {
 // most kNoAllocMaxBlocks blocks: N <= 8,388,608 Gaussians, 128 KiB of scratch. Every GPU that
 // loads the library holds the array until the process exits. All calls share it. A call
 // writes the partial of every block it launches before reading it, so nothing needs clearing
-// between calls. Two calls that overlap on the GPU (unordered streams) race on it.
+// between calls. Two calls that overlap on the GPU (unordered streams) race on it. The array's
+// device address is looked up once per device and kept, so the library must not be used across
+// a cudaDeviceReset (which unloads it from the device). With N = 0 the result is the empty box,
+// lo = +3e38 and hi = -3e38 on every axis, which clips every ray to an empty interval.
 namespace {
 
 constexpr int kNoAllocItemsPerBlock = 2048;
@@ -467,15 +472,17 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) float4 g_noalloc_partial[2 * kNoAllocMaxBlocks];
 
-// the instance AABB of k_prep (8 transformed corners of [-1,1]^3), computed in place
+// the instance AABB of k_prep (8 transformed corners of [-1,1]^3), computed in place from the
+// attributes as the tracer stores them (rounded to 16 bits with BF16 / FP16 storage, as k_prep does)
 __device__ void instance_aabb(int g, const float* __restrict__ pos, const float* __restrict__ rot,
                               const float* __restrict__ scl, const float* __restrict__ dns, const AccelBuildOptions& opt,
                               float3& lo, float3& hi) {
-    const float4 q = make_float4(rot[4 * g], rot[4 * g + 1], rot[4 * g + 2], rot[4 * g + 3]);
+    const auto in = [&](const float* v, int i) { return round_storage(opt.storage, v[i]); };
+    const float4 q = make_float4(in(rot, 4 * g), in(rot, 4 * g + 1), in(rot, 4 * g + 2), in(rot, 4 * g + 3));
     const Mat3 R = quat_r(q);
-    const float ks = support_scale(dns[g], opt.min_response, opt.density_clamping, opt.kernel_degree);
-    const float3 k = make_float3(scl[3 * g], scl[3 * g + 1], scl[3 * g + 2]) * ks;
-    const float3 mu = make_float3(pos[3 * g], pos[3 * g + 1], pos[3 * g + 2]);
+    const float ks = support_scale(in(dns, g), opt.min_response, opt.density_clamping, opt.kernel_degree);
+    const float3 k = make_float3(in(scl, 3 * g), in(scl, 3 * g + 1), in(scl, 3 * g + 2)) * ks;
+    const float3 mu = make_float3(in(pos, 3 * g), in(pos, 3 * g + 1), in(pos, 3 * g + 2));
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
         const float3 corner = make_float3((c & 4) ? 1.0f : -1.0f, (c & 2) ? 1.0f : -1.0f, (c & 1) ? 1.0f : -1.0f);
@@ -515,9 +522,14 @@ void set_error(char* buf, int len, const std::string& msg) {
 }  // namespace ptir
 
 extern "C" int ptir_instance_bounds_noalloc(float kernel_degree, float kernel_min_response, int32_t density_clamping,
-                                            const float* pos, const float* rot, const float* scl, const float* dns,
-                                            int32_t n, float* bounds_out, void* stream, char* err, int32_t err_len) {
+                                            int32_t storage, const float* pos, const float* rot, const float* scl,
+                                            const float* dns, int32_t n, float* bounds_out, void* stream, char* err,
+                                            int32_t err_len) {
     using namespace ptir;
+    if (storage != PTIR_STORAGE_FP32 && storage != PTIR_STORAGE_BF16 && storage != PTIR_STORAGE_FP16) {
+        set_error(err, err_len, "storage must be PTIR_STORAGE_FP32, _BF16 or _FP16");
+        return PTIR_EINVAL;
+    }
     if (n < 0) {
         set_error(err, err_len, "negative Gaussian count");
         return PTIR_EINVAL;
@@ -537,9 +549,14 @@ extern "C" int ptir_instance_bounds_noalloc(float kernel_degree, float kernel_mi
     }
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    if (e != cudaSuccess) {
         set_error(err, err_len, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
         return PTIR_ECUDA;
+    }
+    if (dev < 0 || dev >= kMaxDevices) {
+        set_error(err, err_len, "device index " + std::to_string(dev) + " exceeds the limit of " +
+                                    std::to_string(kMaxDevices) + " devices");
+        return PTIR_EINVAL;
     }
     float4* scratch = nullptr;
     {
@@ -556,7 +573,7 @@ extern "C" int ptir_instance_bounds_noalloc(float kernel_degree, float kernel_mi
         }
         scratch = g_noalloc_device_ptr[dev];
     }
-    const AccelBuildOptions opt{kernel_degree, kernel_min_response, density_clamping};
+    const AccelBuildOptions opt{kernel_degree, kernel_min_response, density_clamping, (unsigned)storage};
     const cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int blocks = (n + kNoAllocItemsPerBlock - 1) / kNoAllocItemsPerBlock;
     if (blocks > 0) k_bounds_noalloc_partial<<<blocks, kReduceThreads, 0, s>>>(n, pos, rot, scl, dns, opt, scratch);

@@ -41,7 +41,7 @@ struct AccelState {
     size_t sort_temp_bytes = 0;
     size_t capacity = 0;        // Gaussians the buffers can hold
 
-    AccelView view() const { return AccelView{nodes4, leaves, bounds, valid ? n : 0}; }
+    AccelView view() const { return AccelView{nodes4, leaves, bounds, valid ? n : 0, 0.0f}; }
 };
 
 // Build (rebuild != 0 or topology unusable) or refit the structure from per-Gaussian

@@ -187,6 +187,7 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, in
 
     std::memset(&p, 0, sizeof(p));
     p.accel = t->accel.view();
+    p.accel.cull_slack = t->cfg.exact_candidates ? ptir::kCullSlack : 0.0f;
     p.part.density = reinterpret_cast<const float4*>(a->particle_density);
     p.part.material = a->particle_material;
     p.part.sph = a->particle_radiance;
@@ -331,6 +332,7 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     if (config->ray_order != 0 && config->ray_order != 1) return PTIR_EINVAL;
     if (config->grad_sums != 0 && config->grad_sums != 1) return PTIR_EINVAL;
     if (config->grad_aggregate != 0 && config->grad_aggregate != 1) return PTIR_EINVAL;
+    if (config->exact_candidates != 0 && config->exact_candidates != 1) return PTIR_EINVAL;
     if (config->storage != PTIR_STORAGE_FP32 && config->storage != PTIR_STORAGE_BF16 &&
         config->storage != PTIR_STORAGE_FP16)
         return PTIR_EINVAL;

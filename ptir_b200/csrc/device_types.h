@@ -10,7 +10,8 @@ namespace ptir {
 // Acceleration structure over the Gaussians' instance boxes. The LBVH is built binary and
 // traversed 4-wide: every binary node at even depth becomes a 4-wide node holding the boxes of
 // its (up to four) grandchildren, so one 128-byte fetch tests four boxes.
-//   node4 = 8 x float4: lo.x[4] lo.y[4] lo.z[4] hi.x[4] hi.y[4] hi.z[4] child[4] (unused);
+//   node4 = 8 x float4: lo.x[4] lo.y[4] lo.z[4] hi.x[4] hi.y[4] hi.z[4] child[4] kmax[4]
+//           (kmax: the largest kernel support radius of any Gaussian under the child);
 //           a child c >= 0 is a 4-wide node, kNoChild an empty slot, any other c < 0 leaf ~c.
 //   leaf  = 4 x float4: rows of the world->instance affine map [A | b] (A = diag(1/k) R^T,
 //           b = -A mu, k = kernel support scale per axis), then (gaussian id, kmax, 0, 0).
@@ -23,7 +24,19 @@ struct AccelView {
     const float4* leaves;
     const float4* bounds;  // [2]: scene AABB lo.xyz, hi.xyz (union of the instance AABBs)
     int n;                 // number of Gaussians (leaves)
+    // Subtree culling against the K-th distance t_K. 0: a subtree is culled when the ray enters its
+    // box after t_K, as the reference's traversal culls (order dependent for grazing candidates).
+    // > 0: culled only when no Gaussian under it can have its closest approach t* before t_K,
+    // using t* >= box entry - kCullSlack * kmax / |d| (exact K-nearest candidates).
+    float cull_slack;
 };
+
+// A ray that hits a Gaussian's instance box [-1,1]^3 and misses the inscribed unit sphere has
+// its closest approach (in instance units) at distance p in [1, sqrt(3)] from the centre, and the
+// box entry lies at most sqrt(3 - p^2) <= sqrt(2) instance units past it along the ray; one
+// instance unit is at most kmax / |d| of the ray parameter. (A ray through the sphere has t* in
+// the box.) With a margin for rounding:
+constexpr float kCullSlack = 1.4143f;
 
 struct EnvView {
     const float4* data;  // [h, w] RGBA texels, null when absent

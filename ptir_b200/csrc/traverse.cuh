@@ -7,13 +7,16 @@
 // (tmin, tend), ascending. A Gaussian is a candidate when its object-space ray hits the unit
 // instance box [-1,1]^3 within [tmin, tend] and passes the perpendicular-distance test.
 //
-// Culling follows the reference's traversal: subtrees are culled by their instance-box AABBs
-// against [tmin, t_K], where t_K is the K-th distance found so far (the reference's any-hit
-// program shrinks the ray's tmax to the 16th distance). This returns the K nearest candidates
-// except for a Gaussian whose closest approach lies before its own box entry (a ray grazing a
-// box corner): like the reference, it is then kept only if reached before t_K drops below its
-// box entry. Its response can pass the acceptance threshold, so K (which sets t_K) can change
-// the image; K = 16 is the reference's.
+// Culling (AccelView::cull_slack = 0) follows the reference's traversal: subtrees are culled by
+// their instance-box AABBs against [tmin, t_K], where t_K is the K-th distance found so far (the
+// reference's any-hit program shrinks the ray's tmax to the 16th distance). This returns the K
+// nearest candidates except for a Gaussian whose closest approach lies before its own box entry
+// (a ray grazing a box corner): like the reference, it is then kept only if reached before t_K
+// drops below its box entry, which depends on the traversal order. Its response can pass the
+// acceptance threshold, so K (which sets t_K) and the order can change the image. With
+// cull_slack > 0 a subtree is culled only when its box entry, less kCullSlack times the largest
+// kernel support radius under it over |d|, lies past t_K: a lower bound of every t* under it, so
+// a call returns exactly the K nearest candidates, whatever the order or K.
 #pragma once
 
 #include "device_types.h"
@@ -84,8 +87,21 @@ PTIR_DEV float min3f(float a, float b, float c) {
     return r;
 }
 
+// The instance intersection of the reference (intersectInstanceParticle,
+// gaussianParticles.cuh:484-500) for the object-space ray (od, dd): the closest approach to the
+// centre t* = -(od . dd) / |dd|^2 within (tmin, tmax), at a squared distance (over |dd|^2) below 9.
+PTIR_DEV bool instance_hit(float3 od, float3 dd, float tmin, float tmax, float& ts) {
+    const float den = 1.0f / dot(dd, dd);
+    ts = -dot(od, dd) * den;
+    if (!(ts > tmin && ts < tmax)) return false;
+    const float3 c = cross(normalize_or_keep(dd), od);
+    return dot(c, c) * den < 9.0f;
+}
+
 // Exact instance test of leaf record p against ray (o, d) over (tmin, min(tend, cut)): true with
-// the candidate's distance and Gaussian id when it is one.
+// the candidate's distance and Gaussian id when it is one. The reference's any-hit traversal
+// invokes its intersection program only for instances whose unit box the ray crosses within the
+// current interval, so the box test is part of the candidate test.
 PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float cut,
                              float& ts_out, unsigned& id_out) {
     const float4* rec = A.leaves + 4 * (size_t)p;
@@ -95,17 +111,13 @@ PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, floa
                                   r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
     const float3 dd = make_float3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
                                   r2.x * d.x + r2.y * d.y + r2.z * d.z);
-    const float dd2 = dot(dd, dd);
-    const float den = 1.0f / dd2;
-    const float ts = -dot(od, dd) * den;
-    if (!(ts > tmin && ts < tend && ts < cut)) return false;
+    float ts;
+    if (!instance_hit(od, dd, tmin, fminf(tend, cut), ts)) return false;
     // object-space unit box within [tmin, tend]
     const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float b0, b1;
     slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
     if (fmaxf(b0, tmin) > fminf(b1, tend)) return false;
-    const float3 c = cross(normalize_or_keep(dd), od);
-    if (!(dot(c, c) * den < 9.0f)) return false;
     ts_out = ts;
     id_out = __float_as_uint(__ldg(&rec[3].x));
     return true;
@@ -125,6 +137,7 @@ PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmi
 struct TraceState {
     float3 inv;
     float tmin, tend;
+    float slack;  // cull_slack / |d|: a child's cull distance is its box entry less slack * its kmax
     int node, sp;
 };
 
@@ -145,6 +158,7 @@ PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, fl
     t.inv = make_float3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     t.tmin = tmin;
     t.tend = tend;
+    t.slack = A.cull_slack > 0.0f ? A.cull_slack / sqrtf(dot(d, d)) : 0.0f;
     t.node = 0;
     t.sp = 0;
     return true;
@@ -154,8 +168,8 @@ PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, fl
 // tested in between (in the lane, or by the whole warp).
 struct NodeVisit {
     int ch[4];           // children: >= 0 node, kNoChild empty, else leaf ~c
-    float t0[4], key[4]; // clipped entry distance, middle of the clipped interval (x2)
-    unsigned hits;       // children whose box the ray crosses in front of the K-th distance
+    float t0[4], key[4]; // cull distance (clipped entry, less the slack), middle of the clipped interval (x2)
+    unsigned hits;       // children whose box the ray crosses and whose cull distance is before t_K
 };
 
 // Box tests of the node t.node. Returns the mask of leaf children to test.
@@ -172,6 +186,11 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, const TraceState& t, 
     const float4 nx = __ldg(nd + rx), ny = __ldg(nd + ry), nz = __ldg(nd + rz);
     const float4 fx = __ldg(nd + (3 - rx)), fy = __ldg(nd + (5 - ry)), fz = __ldg(nd + (7 - rz));
     const float4 cc = __ldg(nd + 6);
+    float sl[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (t.slack > 0.0f) {
+        const float4 km = __ldg(nd + 7);
+        sl[0] = km.x * t.slack; sl[1] = km.y * t.slack; sl[2] = km.z * t.slack; sl[3] = km.w * t.slack;
+    }
     const float nxa[4] = {nx.x, nx.y, nx.z, nx.w}, nya[4] = {ny.x, ny.y, ny.z, ny.w};
     const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fxa[4] = {fx.x, fx.y, fx.z, fx.w};
     const float fya[4] = {fy.x, fy.y, fy.z, fy.w}, fza[4] = {fz.x, fz.y, fz.z, fz.w};
@@ -191,11 +210,11 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, const TraceState& t, 
                               fmaxf(fmaf(nza[k], inv.z, -oi.z), tmin));
         const float b = min3f(fmaf(fxa[k], inv.x, -oi.x), fmaf(fya[k], inv.y, -oi.y),
                               fminf(fmaf(fza[k], inv.z, -oi.z), tend));
-        v.t0[k] = a;
+        v.t0[k] = a - sl[k];
         // nearer middle of the clipped interval first: boxes that contain the origin all
         // enter at tmin, their extent along the ray tells them apart
         v.key[k] = a + b;
-        const bool h = v.ch[k] != kNoChild && a <= b && a <= kt[K - 1];
+        const bool h = v.ch[k] != kNoChild && a <= b && v.t0[k] <= kt[K - 1];
         v.hits |= h ? (1u << k) : 0u;
         leaves |= (h && v.ch[k] < 0) ? (1u << k) : 0u;
     }

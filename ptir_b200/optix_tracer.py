@@ -106,7 +106,10 @@ class OptixTracer:
     and widened on load, all arithmetic staying FP32. ``warp_aggregate`` sums the gradient terms
     that lanes of a warp add to the same Gaussian or texel before the atomics (off: one atomic
     per lane and term). ``shadow_kbuffer`` (8, 16 or 32; 0 = 16) sets the k-buffer of the NEE
-    shadow rays apart from ``kbuffer``."""
+    shadow rays apart from ``kbuffer``. ``exact_candidates`` makes every traversal return exactly
+    the K nearest candidates (off: subtrees are culled by their box entry as the reference's
+    traversal culls them, which keeps a grazing Gaussian or not depending on the order), so that
+    the results depend on neither the traversal order nor ``kbuffer``."""
 
     def __init__(
         self,
@@ -137,6 +140,7 @@ class OptixTracer:
         storage: str = "fp32",
         warp_aggregate: bool = True,
         shadow_kbuffer: int = 0,
+        exact_candidates: bool = False,
     ):
         if pipeline not in ("reference",):
             raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
@@ -153,7 +157,7 @@ class OptixTracer:
             int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
             N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
             int(bool(collect_timings)), 0 if sort_rays else 1, int(bool(exact_replay)), 0 if compensated_grads else 1,
-            N.STORAGES[storage], 0 if warp_aggregate else 1, int(shadow_kbuffer))
+            N.STORAGES[storage], 0 if warp_aggregate else 1, int(shadow_kbuffer), int(bool(exact_candidates)))
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:

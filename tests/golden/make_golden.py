@@ -9,7 +9,7 @@
                      from the reference's own threedgrut/model/light.py (its image-loading import,
                      imageio, is absent here and unused by these functions, so it is stubbed)
 
-Usage: python tests/golden/make_golden.py [--reference /root/reference]
+Usage: python tests/golden/make_golden.py --reference REFERENCE_CHECKOUT   (or $PTIR_REFERENCE_ROOT)
 """
 import argparse
 import importlib.util
@@ -152,7 +152,8 @@ def oracle_small():
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=os.environ.get("PTIR_REFERENCE_ROOT"),
+                    help="the reference checkout (default: $PTIR_REFERENCE_ROOT)")
     a = ap.parse_args()
     sampler_kat(a.reference)
     alias_tables(a.reference)

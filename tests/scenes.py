@@ -129,3 +129,21 @@ def gpu_trace_bwd(tr, S: dict, fwd, pbr_grad, light_grad=None, material_grad=Non
                         S["alias_table"], *_light_tensors(S), z(rad), z(dns), z(hit), z(hit2), z(dist), z(nrm), z(snrm),
                         material_grad, pbr_grad, light_grad, S["render_opts"], S["sph_degree"], S["min_transmittance"],
                         S["max_bounces"])
+
+
+def workload_scene(name: str, view: int = 0, frame: int = 0) -> dict:
+    """The scene dict (as small_scene returns) of one view of a named benchmark workload
+    (ptir_b200/synthetic.py), with the benchmark's generator, camera, environment and alias table."""
+    wl = synthetic.workload(name)
+    f = synthetic.make_field(wl.n, seed=wl.seed, layout=wl.layout, scale_range=wl.scale_range, sh_full=wl.sh_full)
+    w, h, spp = wl.views[view]
+    eye = synthetic.camera_positions(len(wl.views), seed=wl.seed)[view]
+    o, d = synthetic.view_rays(w, h, spp, eye)
+    env = synthetic.make_environment(*wl.env_hw, seed=wl.seed)
+    return dict(
+        build_pos=f["pos"].numpy(), build_rot=f["rot"].numpy(), build_scl=f["scl"].numpy(), build_dns=f["dns"].numpy(),
+        density=synthetic.density_tensor(f).numpy(), material=synthetic.material_tensor(f).numpy(),
+        sph=f["sph"].numpy(), shading_normal=f["snrm"].numpy(), ray_ori=o.numpy(), ray_dir=d.numpy(),
+        ray_to_world=np.eye(4, dtype=np.float32)[None], frame=frame, sph_degree=3, min_transmittance=0.001,
+        max_bounces=wl.max_bounces, render_opts=0, environment=env.numpy(),
+        alias_table=envmap.pack(envmap.build(env)).numpy())

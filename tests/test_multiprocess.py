@@ -54,3 +54,18 @@ def test_gradient_allreduce_gloo_world2():
     for r in (0, 1):
         assert torch.equal(res[r][1], torch.full((5, 5), 3.0))
         assert torch.equal(res[r][2], torch.arange(12, dtype=torch.float32).reshape(1, 3, 4) * 3)
+
+
+def test_weighted_shards_balance_segments():
+    from ptir_b200.dist import shard_weighted
+
+    w = [256 * 256, 800 * 800 * 16, 400 * 400 * 2, 512 * 512 * 4, 800 * 800, 256 * 256 * 16, 512 * 512, 400 * 400]
+    for world in (1, 2, 3, 4, 8):
+        got = [shard_weighted(w, r, world) for r in range(world)]
+        assert sorted(i for g in got for i in g) == list(range(len(w)))
+        loads = [sum(w[i] for i in g) for g in got]
+        # largest-first greedy: within 4/3 of the best (>= max(total / world, largest item))
+        assert max(loads) <= 4.0 / 3.0 * max(sum(w) / world, max(w)) + 1e-9
+    assert shard_weighted([1.0] * 8, 0, 2) == [0, 2, 4, 6]
+    with pytest.raises(ValueError):
+        shard_weighted([1.0, -1.0], 0, 2)
