@@ -22,10 +22,11 @@
  *     tensorBuffering.h:30-39). The per-sample inputs (ray origins and directions, and the
  *     backward's saved outputs and incoming gradients) may be strided, as the reference reads
  *     them through PackedTensorAccessor32 (tensorBuffering.h:41-45, optixTracer.cpp:963-964,
- *     1082-1113): each has a `*_strides[4]` field, the element strides of its [Z,H,W,C] index
- *     (z, y, x, c), any of them 0 for a broadcast dimension; all four 0 means C-contiguous. In
- *     the batched entry points (ptir_trace_views) the per-sample arrays are flat [T,C]: element
- *     (t, c) lies at t * strides[2] + c * strides[3], strides[0] and [1] are unused. Output
+ *     1082-1113): with `use_strides` set in the args struct, each has a `*_strides[4]` field,
+ *     the element strides of its [Z,H,W,C] index (z, y, x, c), 0 for a broadcast dimension; with
+ *     `use_strides` 0 they are C-contiguous and the stride fields are ignored. In the batched
+ *     entry points (ptir_trace_views) the per-sample arrays are flat [T,C]: element (t, c) lies
+ *     at t * strides[2] + c * strides[3], strides[0] and [1] are unused. Output
  *     buffers need no initialisation: every element is written (the reference's zero-filled
  *     outputs are written as zeros).
  *   - The library owns its acceleration structure and scratch; buffers grow, never shrink.
@@ -152,7 +153,9 @@ typedef struct ptir_trace_args {
     int32_t sph_eval_degree;        /* SH degree evaluated (<= sph_degree) */
     float min_transmittance;        /* render.min_transmittance */
     uint32_t max_bounces;           /* render.max_bounces */
-    int64_t ray_origin_strides[4];    /* element strides of ray_origin (see Conventions); 0s: contiguous */
+    int32_t use_strides;              /* 1: ray_origin / ray_direction are read with the strides below, 0: they
+                                         are C-contiguous (see Conventions) */
+    int64_t ray_origin_strides[4];    /* element strides of ray_origin */
     int64_t ray_direction_strides[4]; /* element strides of ray_direction */
 } ptir_trace_args;
 
@@ -188,7 +191,9 @@ typedef struct ptir_bwd_args {
     const float* pbr_grad;        /* [Z,H,W,3] */
     const float* light_grad;      /* [Z,H,W,3] */
     const float* material_grad;   /* [Z,H,W,5] */
-    /* element strides of the five arrays above (see Conventions); all 0: contiguous */
+    /* 1: the five arrays above are read with these element strides, 0: they are C-contiguous (see
+     * Conventions) */
+    int32_t use_strides;
     int64_t pbr_strides[4], light_strides[4], pbr_grad_strides[4], light_grad_strides[4], material_grad_strides[4];
 } ptir_bwd_args;
 

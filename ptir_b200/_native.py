@@ -92,6 +92,7 @@ class PtirTraceArgs(C.Structure):
         ("sph_eval_degree", C.c_int32),
         ("min_transmittance", C.c_float),
         ("max_bounces", C.c_uint32),
+        ("use_strides", C.c_int32),
         ("ray_origin_strides", C.c_int64 * 4),
         ("ray_direction_strides", C.c_int64 * 4),
     ]
@@ -106,6 +107,7 @@ class PtirTraceOutputs(C.Structure):
 
 class PtirBwdArgs(C.Structure):
     _fields_ = [(k, _FP) for k in ("pbr", "light", "pbr_grad", "light_grad", "material_grad")] + [
+        ("use_strides", C.c_int32)] + [
         (k + "_strides", C.c_int64 * 4) for k in ("pbr", "light", "pbr_grad", "light_grad", "material_grad")]
 
 

@@ -109,11 +109,11 @@ unsigned flags_of(const ptir_config& c) {
     return f;
 }
 
-// Element strides of a per-sample array from the caller's (all zero: C-contiguous with `channels`
-// channels); false for a negative stride. `flat`: the batched [T,C] form, where only the sample
-// stride (strides[2]) and the channel stride (strides[3]) apply.
-bool sample_layout(const int64_t* s, int channels, int h, int w, bool flat, ptir::SampleLayout& L) {
-    if (s[0] == 0 && s[1] == 0 && s[2] == 0 && s[3] == 0) {
+// Element strides of a per-sample array: the caller's when `strided`, else C-contiguous with
+// `channels` channels; false for a negative stride. `flat`: the batched [T,C] form, where only the
+// sample stride (strides[2]) and the channel stride (strides[3]) apply.
+bool sample_layout(bool strided, const int64_t* s, int channels, int h, int w, bool flat, ptir::SampleLayout& L) {
+    if (!strided) {
         L.sc = 1;
         L.sx = channels;
         L.sy = flat ? 0 : (long long)channels * w;
@@ -227,8 +227,9 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, in
     p.ray_ori = a->ray_origin;
     p.ray_dir = a->ray_direction;
     p.flat_samples = flat ? 1 : 0;
-    if (!sample_layout(a->ray_origin_strides, 3, a->h, a->w, flat, p.ray_ori_layout) ||
-        !sample_layout(a->ray_direction_strides, 3, a->h, a->w, flat, p.ray_dir_layout))
+    const bool rs = a->use_strides != 0;
+    if (!sample_layout(rs, a->ray_origin_strides, 3, a->h, a->w, flat, p.ray_ori_layout) ||
+        !sample_layout(rs, a->ray_direction_strides, 3, a->h, a->w, flat, p.ray_dir_layout))
         return fail(t, PTIR_EINVAL, "negative ray stride");
     long long offset = 0, tile0 = 0;
     for (int v = 0; v < nviews; ++v) {
@@ -464,11 +465,12 @@ int trace_bwd_impl(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* vi
     bi.light_grad = b->light_grad;
     bi.material_grad = b->material_grad;
     const bool flat = views != nullptr;
-    if (!sample_layout(b->pbr_strides, 3, a->h, a->w, flat, bi.pbr_layout) ||
-        !sample_layout(b->light_strides, 3, a->h, a->w, flat, bi.light_layout) ||
-        !sample_layout(b->pbr_grad_strides, 3, a->h, a->w, flat, bi.pbr_grad_layout) ||
-        !sample_layout(b->light_grad_strides, 3, a->h, a->w, flat, bi.light_grad_layout) ||
-        !sample_layout(b->material_grad_strides, 5, a->h, a->w, flat, bi.material_grad_layout))
+    const bool bs = b->use_strides != 0;
+    if (!sample_layout(bs, b->pbr_strides, 3, a->h, a->w, flat, bi.pbr_layout) ||
+        !sample_layout(bs, b->light_strides, 3, a->h, a->w, flat, bi.light_layout) ||
+        !sample_layout(bs, b->pbr_grad_strides, 3, a->h, a->w, flat, bi.pbr_grad_layout) ||
+        !sample_layout(bs, b->light_grad_strides, 3, a->h, a->w, flat, bi.light_grad_layout) ||
+        !sample_layout(bs, b->material_grad_strides, 5, a->h, a->w, flat, bi.material_grad_layout))
         return fail(t, PTIR_EINVAL, "negative stride of a backward input");
     bi.particle_material_grad = o->particle_material_grad;
     bi.environment_grad = env ? o->environment_grad : nullptr;

@@ -43,7 +43,8 @@ def _f32_strided(t: torch.Tensor, name: str) -> torch.Tensor:
 
 
 def _strides4(t: torch.Tensor | None):
-    """The element strides of a [Z,H,W,C] (or [1,1,T,C]) tensor for a `*_strides[4]` field."""
+    """The element strides of a [Z,H,W,C] (or [1,1,T,C]) tensor for a `*_strides[4]` field (an
+    absent tensor's are zeros, unused)."""
     s = (0, 0, 0, 0) if t is None else tuple(int(v) for v in t.stride())
     return (C.c_int64 * 4)(*s)
 
@@ -223,6 +224,7 @@ class OptixTracer:
         a.frame = int(frame) & 0xFFFFFFFF
         a.ray_to_world = _ptr(t2w)
         a.ray_origin, a.ray_direction = _ptr(ori), _ptr(dirs)
+        a.use_strides = 1
         a.ray_origin_strides, a.ray_direction_strides = _strides4(ori), _strides4(dirs)
         a.z, a.h, a.w = int(ori.shape[0]), int(ori.shape[1]), int(ori.shape[2])
         a.particle_density, a.particle_material, a.particle_radiance = _ptr(dens), _ptr(mat), _ptr(rad)
@@ -322,7 +324,7 @@ class OptixTracer:
         snrm_grad = (torch.zeros_like(particle_shading_normal) if particle_shading_normal is not None
                      else torch.zeros((n, 3), dtype=torch.float32, device=dev))
         env_grad = torch.zeros_like(environment)
-        b = N.PtirBwdArgs(_ptr(pbr), _ptr(light), _ptr(pbr_g), _ptr(light_g), _ptr(mat_g), _strides4(pbr),
+        b = N.PtirBwdArgs(_ptr(pbr), _ptr(light), _ptr(pbr_g), _ptr(light_g), _ptr(mat_g), 1, _strides4(pbr),
                           _strides4(light), _strides4(pbr_g), _strides4(light_g), _strides4(mat_g))
         o = N.PtirBwdOutputs(_ptr(material_grad), _ptr(env_grad) if env is not None else None)
         if _views is None:

@@ -218,3 +218,31 @@ def test_paths_with_the_oracles_decisions_match_it(cuda_device, case):
     assert rep["material_rel_l2"] <= 1e-3 and rep["material_cos"] >= 0.999, rep
     assert rep["env_rel_l2"] <= 1e-3 and rep["env_cos"] >= 0.999, rep
 
+
+
+def test_strided_per_sample_inputs_match_contiguous(cuda_device):
+    """Rays and backward inputs are read with their own strides (PackedTensorAccessor32 semantics,
+    tensorBuffering.h:41-45): a ray tensor sliced out of a wider one, and a broadcast (stride 0)
+    pbr gradient as autograd hands it for a mean loss, give the results of contiguous copies, with
+    no copy made (forward bitwise; gradients up to the order of the atomics)."""
+    s = small_scene(n=1500, w=32, h=24, spp=2, max_bounces=3)
+    S = to_torch(s)
+    tr = make_tracer()
+    ref = gpu_trace(tr, S)
+    # rays as strided slices of a [Z,H,W,7] tensor (ray data interleaved with padding)
+    wide = torch.zeros(S["ray_ori"].shape[:3] + (7,), device="cuda")
+    wide[..., 0:3] = S["ray_ori"]
+    wide[..., 4:7] = S["ray_dir"]
+    S2 = dict(S, ray_ori=wide[..., 0:3], ray_dir=wide[..., 4:7])
+    assert not S2["ray_ori"].is_contiguous()
+    got = gpu_trace(tr, S2, build=False)
+    for a, b in zip(ref, got):
+        assert torch.equal(a, b)
+    # a broadcast pbr gradient against its contiguous copy
+    g_b = torch.full((1, 1, 1, 1), 0.25, device="cuda").expand_as(ref[10])
+    assert g_b.stride() == (0, 0, 0, 0)
+    _, mg_b, _, _, eg_b = gpu_trace_bwd(tr, S, ref, g_b)
+    _, mg_c, _, _, eg_c = gpu_trace_bwd(tr, S, ref, g_b.contiguous())
+    assert float(mg_c.abs().sum()) > 0.0
+    assert float((mg_b - mg_c).norm() / mg_c.norm().clamp_min(1e-30)) <= 1e-6
+    assert float((eg_b - eg_c).norm() / eg_c.norm().clamp_min(1e-30)) <= 1e-6
