@@ -32,11 +32,11 @@ struct AccelState {
     unsigned* arrivals = nullptr;  // [n-1] refit arrival counters
     float4* partial = nullptr;  // [kReduceBlocks*2] per-block bounds
     float4* bounds = nullptr;   // [2] scene AABB
-    unsigned* even = nullptr;   // [n-1] 1 where a binary node sits at even depth (a 4-wide node)
-    unsigned* slot4 = nullptr;  // [n-1] index of that 4-wide node
+    int* wroot = nullptr;       // [n-1] binary node at the root of each 4-wide node
+    int* wsrc = nullptr;        // [(n-1)*4] children of each 4-wide node as binary references (refits)
+    int* wchild = nullptr;      // [(n-1)*4] the same children as 4-wide node indices or leaves
+    unsigned* wcount = nullptr; // number of 4-wide nodes
     float4* nodes4 = nullptr;   // [(n-1)*8] 4-wide nodes traversed by the tracer
-    void* scan_temp = nullptr;
-    size_t scan_temp_bytes = 0;
     void* sort_temp = nullptr;
     size_t sort_temp_bytes = 0;
     size_t capacity = 0;        // Gaussians the buffers can hold

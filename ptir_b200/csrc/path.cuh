@@ -206,7 +206,7 @@ PTIR_DEV bool shadow_occluded(const Ctx& C, float3 o, float3 d, float tmax, Pcg3
             const float alpha = (r.gres > P.min_response && r.alpha > P.alpha_min) ? r.alpha : 0.0f;
             if (alpha > 0.0f && rng.uniform() < alpha) return true;
         }
-        if (batch_end <= start) break;
+        if (batch_end <= start || kid[Ctx::K - 1] == kNoHit) break;
         start = batch_end;
     }
     return false;
@@ -578,6 +578,19 @@ PTIR_DEV void composite_hits_strided(const TraceParams& P, TraceCounters& ctr, C
     }
 }
 
+// Composite entries [from, to) of a batch held in memory whose entries are leaf-record indices
+// (k-buffers filled with kLeafIndex).
+template <bool kSelfOcc>
+PTIR_DEV void composite_leaf_batch(const TraceParams& P, TraceCounters& ctr, Composite& c, const float* kt,
+                                   const unsigned* kp, int stride, int from, int to, float* vis) {
+#pragma unroll 1
+    for (int i = from; i < to; ++i) {
+        const unsigned p = kp[i * stride];
+        if (p == kNoHit) break;
+        composite_one<kSelfOcc>(P, ctr, c, kt[i * stride], leaf_gaussian(P.accel, p), vis);
+    }
+}
+
 // The segment after compositing: every field reset but the MIS pdfs (kept when MIS is on),
 // the interaction when the segment is opaque enough, else the escape draw.
 PTIR_DEV void composite_end(const TraceParams& P, const Composite& c, float scatter_pdf, float light_pdf, Segment& s,
@@ -625,6 +638,8 @@ PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
                    C.ctr);
         if (kid[0] == kNoHit) break;
         composite_hits<kSelfOcc>(P, C.ctr, c, kt, kid, vis);
+        // a k-buffer that is not full held every candidate of the call: a later call finds none
+        if (kid[Ctx::K - 1] == kNoHit) break;
     }
     composite_end(P, c, s.scatter_pdf, s.light_pdf, s, rng);
 }
@@ -771,6 +786,7 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const Repla
         trace_kbuf(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
         replay_batch(P, B, r, kt, kid, C.ctr);
+        if (kid[Ctx::K - 1] == kNoHit) break;
     }
 }
 

@@ -123,13 +123,34 @@ PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, floa
     return true;
 }
 
-// exact instance test of leaf record p, inserted into the k-buffer when it is a candidate
-template <int K, class Ids>
+// exact instance test of leaf record p, inserted into the k-buffer when it is a candidate: as its
+// Gaussian id, or with kLeafIndex as the leaf record's index (leaf_gaussian maps it to the id)
+template <int K, bool kLeafIndex = false, class Ids>
 PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
                         Ids& kid) {
     float ts;
     unsigned gid;
-    if (leaf_candidate(A, p, o, d, tmin, tend, kt[K - 1], ts, gid)) kbuf_insert(kt, kid, ts, gid);
+    if (leaf_candidate(A, p, o, d, tmin, tend, kt[K - 1], ts, gid)) kbuf_insert(kt, kid, ts, kLeafIndex ? (unsigned)p : gid);
+}
+
+// Gaussian id of leaf record p
+PTIR_DEV unsigned leaf_gaussian(const AccelView& A, unsigned p) { return __float_as_uint(__ldg(&A.leaves[4 * (size_t)p + 3].x)); }
+
+// Whether the ray crosses the unit instance box of leaf record p within [tmin, tend]: the part of the
+// candidate test that depends on the call's interval (a candidate of an earlier call that passes it
+// with a later tmin is a candidate of that later call too)
+PTIR_DEV bool leaf_box_hit(const AccelView& A, unsigned p, float3 o, float3 d, float tmin, float tend) {
+    const float4* rec = A.leaves + 4 * (size_t)p;
+    const float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
+    const float3 od = make_float3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w,
+                                  r1.x * o.x + r1.y * o.y + r1.z * o.z + r1.w,
+                                  r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
+    const float3 dd = make_float3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
+                                  r2.x * d.x + r2.y * d.y + r2.z * d.z);
+    const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+    float b0, b1;
+    slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
+    return fmaxf(b0, tmin) <= fminf(b1, tend);
 }
 
 // A trace call in progress: the next node to visit and the stack depth (the stack itself is
@@ -143,7 +164,7 @@ struct TraceState {
 
 // Start a trace call of ray (o, d) over (tmin, tend). Returns true when node visits remain
 // (trace_step), false when (kt, kid) is already final.
-template <int K, class Ids>
+template <int K, bool kLeafIndex = false, class Ids>
 PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K], Ids& kid,
                           TraceState& t, TraceCounters& ctr) {
     kbuf_clear(kt, kid);
@@ -151,7 +172,7 @@ PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, fl
     if (A.n <= 0) return false;
     if (A.n == 1) {
         ++ctr.leaves;
-        test_leaf(A, 0, o, d, tmin, tend, kt, kid);
+        test_leaf<K, kLeafIndex>(A, 0, o, d, tmin, tend, kt, kid);
         ctr.candidates += kbuf_count(kt);
         return false;
     }
@@ -285,7 +306,7 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
 
 // One 4-wide node visit of a trace call with its leaf tests in the lane. Returns false when the
 // call is complete.
-template <int K, class Ids>
+template <int K, bool kLeafIndex = false, class Ids>
 PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid, int* stack,
                          float* stack_t, unsigned* err, TraceCounters& ctr) {
     NodeVisit v;
@@ -296,7 +317,7 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
         leaves &= leaves - 1;
         const int c = k == 0 ? v.ch[0] : (k == 1 ? v.ch[1] : (k == 2 ? v.ch[2] : v.ch[3]));
         ++ctr.leaves;
-        test_leaf(A, ~c, o, d, t.tmin, t.tend, kt, kid);
+        test_leaf<K, kLeafIndex>(A, ~c, o, d, t.tmin, t.tend, kt, kid);
     }
     if (descend(t, v, kt, stack, stack_t, err, ctr)) return true;
     ctr.candidates += kbuf_count(kt);
