@@ -75,10 +75,13 @@ typedef struct ptir_config {
     int32_t schedule;             /* PTIR_SCHEDULE_WAVEFRONT (default) or PTIR_SCHEDULE_MEGAKERNEL */
     int32_t chunk_tiles;          /* wavefront: 8x4 pixel tiles per chunk of paths (0 = sized at the tracer's
                                      first trace to a third of the free device memory, at least 32768) */
-    int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16, the
-                                     reference's). Another size culls subtrees at another distance and
-                                     keeps another set of grazing candidates (closest approach before
-                                     their box entry), which changes a small share of the samples. */
+    int32_t kbuffer;              /* wavefront: candidates gathered per traversal, 8, 16 or 32 (0 = 16).
+                                     Segments are composited in the reference's rounds of 16 candidates
+                                     with 16 and 32: a 32-entry traversal stands for two rounds when its
+                                     second half is exactly the next round's candidates, else the next
+                                     round is traced. 8 composites in rounds of 8, which changes a small
+                                     share of the samples (a round's candidates must have their box
+                                     crossed within the round's interval). */
     int32_t refill_lanes;         /* wavefront intersection: waiting lanes, 1..32, before a warp refills (0 = 32) */
     int32_t block_size;           /* wavefront: threads per block, 64, 128 or 256 (0 = 128) */
     int32_t collect_timings;      /* record CUDA events around every kernel launch (ptir_get_stage_times) */

@@ -94,7 +94,8 @@ class OptixTracer:
     The keyword arguments after the reference's own set the B200 launch shape (no counterpart in
     the reference): ``schedule`` ("wavefront" or "megakernel"), and for the wavefront
     ``chunk_tiles`` (8x4 pixel tiles per chunk), ``kbuffer`` (8, 16 or 32 candidates per
-    traversal), ``refill_lanes`` (waiting lanes before an intersection warp refills, 1..32) and
+    traversal; 16 and 32 composite in the reference's rounds of 16, a 32-entry traversal standing
+    for two rounds when its second half is the next round's candidates), ``refill_lanes`` (waiting lanes before an intersection warp refills, 1..32) and
     ``block_size`` (64, 128 or 256); 0 keeps the default. ``collect_timings`` records CUDA events
     around every kernel launch for ``stage_times()``; ``sort_rays`` intersects bounce rays in
     (direction octant, origin cell, direction cell) order (the results do not change); ``exact_replay`` lets the

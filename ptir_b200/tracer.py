@@ -70,12 +70,52 @@ def _make_filter(kind):
         return _AtrousFilter(kind)
 
 
+_MASK_APPLIED_KEY = "_pbr_gt_mask_applied"
+_MASKED_KEYS = ("pred_light", "pred_shadingnormal", "pred_material")
+
+
+def _apply_mask(t, mask):
+    """An NHWC image times the batch's foreground mask broadcast to it
+    (threedgrut/model/ptir_helper.py:64-97)."""
+    if t is None or mask is None or t.ndim != 4:
+        return t
+    m = mask.detach().to(device=t.device, dtype=t.dtype).clamp(0.0, 1.0)
+    if m.ndim == 2:
+        m = m[None, :, :, None]
+    elif m.ndim == 3:
+        m = m.unsqueeze(0) if (m.shape[-1] == 1 and m.shape[:2] == t.shape[1:3]) else m.unsqueeze(-1)
+    elif m.ndim != 4:
+        raise ValueError(f"GT mask must be 2D, 3D, or 4D, got {m.ndim}D")
+    if m.shape[-1] != 1:
+        m = m[..., :1]
+    if m.shape[0] == 1 and t.shape[0] != 1:
+        m = m.expand(t.shape[0], -1, -1, -1)
+    if m.shape[:3] != t.shape[:3]:
+        raise ValueError(f"GT mask shape {tuple(m.shape)} is not compatible with {tuple(t.shape)}")
+    return t * m
+
+
 def _post_processing(outputs, batch, visualize_lights):
+    """Masks the light, shading-normal and material images with the batch's foreground mask
+    (threedgrut/model/ptir_helper.py:100-122); threedgrut's own function when it is importable."""
     try:
         from threedgrut.model.ptir_helper import post_processing  # type: ignore
     except Exception:
+        post_processing = None
+    if post_processing is not None:
+        return post_processing(outputs, batch, visualize_lights)
+    mask = getattr(batch, "mask", None)
+    if bool(outputs.get(_MASK_APPLIED_KEY, False)) or mask is None:
         return outputs
-    return post_processing(outputs, batch, visualize_lights)
+    out = dict(outputs)
+    applied = False
+    for k in _MASKED_KEYS:
+        if outputs.get(k) is not None:
+            out[k] = _apply_mask(outputs[k], mask)
+            applied = True
+    if applied:
+        out[_MASK_APPLIED_KEY] = True
+    return out
 
 
 class _EventTimer:
