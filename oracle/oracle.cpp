@@ -1781,52 +1781,53 @@ int orc_num_threads(void) { return omp_get_max_threads(); }
 // Light samples from positions pos [m,3], sample i drawn from the launch stream (i, 0, 0, frame):
 // out [m,9] = wi xyz, Li rgb, pdf, dist, type; eval_pdf [m] = the light sampler's pdf of the
 // sampled direction (lightSampler.cuh:340-406). FP64.
-// Known-answer evaluations of single reference functions, the cases of tests/golden/device_kat.npz
-// (inputs and outputs laid out as the reference kernels of oracle/ref_device_kat.cu lay them out),
-// in FP64. env_grad [eh, ew, 4] receives the environment gradient of "env_bwd".
-int orc_kat(const orc_config* c, const orc_scene* sc, const char* name, int n, const float* in, double* out,
-            double* env_grad) {
+}  // extern "C"
+
+// Known-answer evaluations of single reference functions in scalar type T (see orc_kat).
+template <class T>
+static int kat_impl(const orc_config* c, const orc_scene* sc, const char* name, int n, const float* in, double* out,
+                    double* env_grad) {
     const Config cfg = to_cfg(c);
     const Inputs inp = to_in(sc);
-    Instances<double> I;
-    build_instances<double>(cfg, inp, I);
-    Tracer<double> tr(cfg, inp, I);
+    Instances<T> I;
+    build_instances<T>(cfg, inp, I);
+    Tracer<T> tr(cfg, inp, I);
     std::vector<double> eg(size_t(std::max(inp.eh, 0)) * std::max(inp.ew, 0) * 4, 0.0);
     tr.env_grad = &eg;
-    using V = V3<double>;
+    using V = V3<T>;
     const std::string what(name);
-    auto v3f = [](const float* p) { return V{double(p[0]), double(p[1]), double(p[2])}; };
+    auto v3f = [](const float* p) { return V{T(p[0]), T(p[1]), T(p[2])}; };
     auto put3 = [](double* o, const V& v) { o[0] = v.x; o[1] = v.y; o[2] = v.z; };
     for (int i = 0; i < n; ++i) {
         if (what == "process_hit") {
             const float* a = in + 8 * size_t(i);
-            Tracer<double>::HitSums h;
+            typename Tracer<T>::HitSums h;
             h.transmittance = a[7];
-            const bool acc = tr.process_hit(uint32_t(a[6]), Ray<double>{v3f(a), v3f(a + 3)}, h);
+            const bool acc = tr.process_hit(uint32_t(a[6]), Ray<T>{v3f(a), v3f(a + 3)}, h);
             double* o = out + 18 * size_t(i);
             o[0] = acc ? 1.0 : 0.0; o[1] = h.transmittance; put3(o + 2, h.radiance); o[5] = h.depth; o[6] = h.depth2;
             put3(o + 7, h.alb); o[10] = h.rgh; o[11] = h.met; put3(o + 12, h.snrm); put3(o + 15, h.normal);
         } else if (what == "intersect") {
             const float* a = in + 8 * size_t(i);
-            double t = 0.0;
-            const bool hit = Tracer<double>::instance_hit(v3f(a), v3f(a + 3), a[6], a[7], t);
+            T t = T(0);
+            const bool hit = Tracer<T>::instance_hit(v3f(a), v3f(a + 3), T(a[6]), T(a[7]), t);
             out[2 * size_t(i)] = hit ? 1.0 : 0.0;
             out[2 * size_t(i) + 1] = t;
         } else if (what == "brdf_sample" || what == "brdf_eval" || what == "brdf_grads") {
             const float* a = in + 16 * size_t(i);
             const V wo = v3f(a), nrm = v3f(a + 3), alb = v3f(a + 6), r3 = v3f(a + 11);
-            double pdf = 0.0;
+            T pdf = T(0);
             if (what == "brdf_eval") {
-                put3(out + 4 * size_t(i), tr.eval_brdf(wo, nrm, alb, a[9], a[10], r3, pdf));
+                put3(out + 4 * size_t(i), tr.eval_brdf(wo, nrm, alb, T(a[9]), T(a[10]), r3, pdf));
                 out[4 * size_t(i) + 3] = pdf;
             } else if (what == "brdf_sample") {
                 V next{};
-                const V v = tr.sample_brdf(wo, nrm, alb, a[9], a[10], r3, next, pdf);
+                const V v = tr.sample_brdf(wo, nrm, alb, T(a[9]), T(a[10]), r3, next, pdf);
                 double* o = out + 7 * size_t(i);
                 put3(o, v); put3(o + 3, next); o[6] = pdf;
             } else {
                 V next{};
-                const BrdfGrad<double> g = tr.sample_brdf_grad(wo, nrm, alb, a[9], a[10], r3, next, pdf);
+                const BrdfGrad<T> g = tr.sample_brdf_grad(wo, nrm, alb, T(a[9]), T(a[10]), r3, next, pdf);
                 double* o = out + 19 * size_t(i);
                 put3(o, g.value); put3(o + 3, g.d_albedo); put3(o + 6, g.d_metallic); put3(o + 9, g.d_roughness);
                 put3(o + 12, g.d_next_dir); put3(o + 15, next); o[18] = pdf;
@@ -1844,7 +1845,7 @@ int orc_kat(const orc_config* c, const orc_scene* sc, const char* name, int n, c
             const float* a = in + 4 * size_t(i);
             Sampler s;
             s.init_launch(unsigned(a[0]), unsigned(a[1]), unsigned(a[2]), unsigned(a[3]));
-            double pdf = 0.0;
+            T pdf = T(0);
             put3(out + 4 * size_t(i), tr.sample_alias_dir(s, pdf));
             out[4 * size_t(i) + 3] = pdf;
         } else if (what == "light_sample") {
@@ -1863,6 +1864,17 @@ int orc_kat(const orc_config* c, const orc_scene* sc, const char* name, int n, c
     }
     if (env_grad) std::copy(eg.begin(), eg.end(), env_grad);
     return 0;
+}
+
+extern "C" {
+
+// Known-answer evaluations of single reference functions, the cases of tests/golden/device_kat.npz
+// (inputs and outputs laid out as the reference kernels of oracle/ref_device_kat.cu lay them out),
+// in FP64, or with fp32 != 0 in the FP32 instantiation. env_grad [eh, ew, 4] receives the
+// environment gradient of "env_bwd".
+int orc_kat(const orc_config* c, const orc_scene* sc, const char* name, int n, const float* in, double* out,
+            double* env_grad, int fp32) {
+    return fp32 ? kat_impl<float>(c, sc, name, n, in, out, env_grad) : kat_impl<double>(c, sc, name, n, in, out, env_grad);
 }
 
 int orc_light_samples(const orc_config* c, const orc_scene* sc, int m, const float* pos, double* out,

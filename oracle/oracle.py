@@ -109,7 +109,7 @@ def lib():
         L.orc_launch_seed.restype = C.c_ulonglong
         L.orc_num_threads.restype = C.c_int
         L.orc_light_samples.argtypes = [P(_Config), P(_Scene), C.c_int, _FP, P(C.c_double), P(C.c_double)]
-        L.orc_kat.argtypes = [P(_Config), P(_Scene), C.c_char_p, C.c_int, _FP, P(C.c_double), P(C.c_double)]
+        L.orc_kat.argtypes = [P(_Config), P(_Scene), C.c_char_p, C.c_int, _FP, P(C.c_double), P(C.c_double), C.c_int]
         _LIB = L
     return _LIB
 
@@ -331,10 +331,10 @@ KAT_COLUMNS = {"process_hit": 18, "intersect": 2, "brdf_sample": 7, "brdf_eval":
                "env_lookup": 4, "env_bwd": 6, "env_sample": 4, "light_sample": 9, "light_pdf": 1}
 
 
-def kat(cfg: OracleConfig, scene: dict, name: str, inputs: np.ndarray):
-    """The oracle's FP64 evaluation of one reference function on known-answer inputs laid out as
-    oracle/ref_device_kat.cu lays them out. Returns (outputs [n, KAT_COLUMNS[name]] f64,
-    environment gradient [eh, ew, 4] f64 of "env_bwd")."""
+def kat(cfg: OracleConfig, scene: dict, name: str, inputs: np.ndarray, precision: str = "f64"):
+    """The oracle's evaluation of one reference function on known-answer inputs laid out as
+    oracle/ref_device_kat.cu lays them out, in FP64 or ("f32") its FP32 instantiation. Returns
+    (outputs [n, KAT_COLUMNS[name]] f64, environment gradient [eh, ew, 4] f64 of "env_bwd")."""
     keep = _Keep()
     s = dict(scene)
     s.setdefault("ray_ori", np.zeros((1, 1, 1, 3), np.float32))
@@ -346,7 +346,7 @@ def kat(cfg: OracleConfig, scene: dict, name: str, inputs: np.ndarray):
     eg = np.zeros((max(sc.eh, 1), max(sc.ew, 1), 4), np.float64)
     P = C.POINTER(C.c_double)
     rc = lib().orc_kat(C.byref(cfg._c()), C.byref(sc), name.encode(), n, _f(x), out.ctypes.data_as(P),
-                       eg.ctypes.data_as(P))
+                       eg.ctypes.data_as(P), 1 if precision == "f32" else 0)
     assert rc == 0, name
     return out, eg[: sc.eh, : sc.ew]
 

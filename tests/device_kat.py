@@ -50,10 +50,49 @@ def oracle_scene(g: dict, scene: str | None) -> dict:
     return {}
 
 
+EPS32 = 2.0 ** -24
+
+# Outputs that are forward differences of float evaluations over eps = 1e-3: the roughness
+# derivative of the sampled direction (material.cuh:30,362-375) and the direction gradient of an
+# environment lookup (environment.cuh:16,421-445). Their rounding error is that of the two
+# evaluations times 1 / eps, so they are compared as vectors (fd_report).
+FD_COLUMNS = {"brdf_grads": slice(12, 15), "env_bwd": slice(3, 6)}
+
+
+def value_columns(entry: str, cols: int) -> list:
+    fd = FD_COLUMNS.get(entry)
+    return [c for c in range(cols) if fd is None or not fd.start <= c < fd.stop]
+
+
+def case_rtol(entry: str, x: np.ndarray, rtol: float) -> np.ndarray:
+    """Per-case relative tolerance: `rtol`, widened for the BRDF functions by the float
+    conditioning of the GGX sampling and distribution at roughness r: 1 + (alpha^2 - 1) u with
+    alpha = max(r, 0.05)^2 keeps only log2(1 / alpha^2) fewer bits (material.cuh:26-27,230-286), so
+    the float result carries about eps32 / alpha^2 of relative error."""
+    if entry.startswith("brdf"):
+        a2 = np.maximum(x[:, 10].astype(np.float64), 0.05) ** 4
+        return rtol + 4.0 * EPS32 / a2
+    return np.full(x.shape[0], rtol)
+
+
 def close(x, ref, atol, rtol):
-    """Per case: every column within atol + rtol * |ref|."""
+    """Per case: every column within atol + rtol * |ref| (rtol a scalar or one per case)."""
     x, ref = np.asarray(x, np.float64), np.asarray(ref, np.float64)
+    rtol = np.asarray(rtol, np.float64)
+    if rtol.ndim == 1:
+        rtol = rtol[:, None]
     return np.all(np.abs(x - ref) <= atol + rtol * np.abs(ref), axis=-1)
+
+
+def fd_report(out, ref) -> dict:
+    """Finite-difference outputs as vectors: relative L2 and cosine over all cases, and the share of
+    cases within 1e-4 + 1e-2 |ref| (vector norms)."""
+    a, b = np.asarray(out, np.float64), np.asarray(ref, np.float64)
+    nb = np.linalg.norm(b)
+    rel = float(np.linalg.norm(a - b) / max(nb, 1e-30))
+    cos = float((a * b).sum() / max(np.linalg.norm(a) * nb, 1e-30))
+    share = float(np.mean(np.linalg.norm(a - b, axis=1) <= 1e-4 + 1e-2 * np.linalg.norm(b, axis=1)))
+    return dict(rel_l2=rel, cos=cos, share=share)
 
 
 class PtirKat:
