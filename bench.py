@@ -318,6 +318,9 @@ def _view_config(views):
 # a material gradient, so the adjoint re-traverses those segments even where no light reaches the
 # camera (the 1M-Gaussian scene's opaque shell keeps its pbr image black).
 LOSS_L1, LOSS_ALBEDO, LOSS_ROUGHNESS = 0.8, 0.5, 0.2
+# dram__bytes_read.sum + dram__bytes_write.sum of k_wf_trace per segment it intersects, from an ncu
+# capture of 16 launches on 2 views of 512x384x4 (1,232,548,608 bytes over ~1,652,977 segments)
+DRAM_BYTES_PER_INTERSECT_SEGMENT = 745.7
 STEP_DESC = ("lbvh refit + forward + loss (0.8 L1(pbr, target) + 0.5 L2(albedo, prior) + 0.2 L2(roughness, prior)) "
              "+ adjoint + selective adam (material, env)")
 
@@ -379,6 +382,8 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, chunk_tiles=args.chunk_tiles)
     if args.exact_candidates:
         shape = dict(shape, exact_candidates=True)
+    if args.resume_rounds is not None:
+        shape = dict(shape, resume_rounds=args.resume_rounds)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     backward = S.wl.backward
@@ -577,6 +582,12 @@ def run_ours(args, rank, world, device):
     dom_ms = dom_ms_total / dom_launches
     peak, peak_kind = _peaks()
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    # DRAM traffic of the intersection kernel per launch, scaled from an ncu capture of a smaller
+    # case by the segments the launch intersects
+    traffic = None
+    if dom == "intersect":
+        isect_segs = fcs[dom].get("segments", 0) + bcs[dom].get("segments", 0)
+        traffic = DRAM_BYTES_PER_INTERSECT_SEGMENT * isect_segs / launches_step
     launches_per_step = ACCEL_KERNELS_PER_BUILD + sum(n for _, n in stage_t.values()) / stage_steps
     h2d = int(S.ray_ori.numel() * 4 * 2)
     res = {
@@ -599,7 +610,7 @@ def run_ours(args, rank, world, device):
         "pass_ms": {"forward": fwd_ms, "backward": bwd_ms},
         "stages_ms_per_step": {KERNEL_OF_STAGE[st]: stage_t[st][0] / stage_steps for st in STAGES if stage_t[st][1]},
         "roofline": {"bound": "hbm", "kernel": KERNEL_OF_STAGE[dom], "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                      "algorithmic_bytes_per_launch": dom_bytes, "ms_per_launch": dom_ms,
                      "launches_per_step": launches_step},
         "counters": {"forward": fc, "backward": bc, "forward_by_stage": fcs, "backward_by_stage": bcs},
@@ -787,6 +798,9 @@ def main():
                     help="one gradient atomic per lane and term (default: warp-aggregated rows)")
     ap.add_argument("--kbuffer", type=int, default=0, choices=(0, 8, 16, 24, 32),
                     help="candidates per traversal (0: the tuned or default size)")
+    ap.add_argument("--resume-rounds", type=int, choices=(0, 1, 2), default=None,
+                    help="k-buffer rounds resumed from the previous round's frontier: 0 backward replay (default), "
+                         "1 none, 2 replay and intersection")
     ap.add_argument("--exact-candidates", action="store_true",
                     help="every traversal returns exactly the K nearest candidates (order independent)")
     args = ap.parse_args()

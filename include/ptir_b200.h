@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define PTIR_ABI_VERSION 4
+#define PTIR_ABI_VERSION 5
 
 enum {
     PTIR_OK = 0,
@@ -113,6 +113,12 @@ typedef struct ptir_config {
                                      approach under them can lie before the K-th distance), so the results
                                      depend on neither the order nor the k-buffer size (no counterpart in
                                      the reference) */
+    int32_t resume_rounds;        /* wavefront, k-buffer 8 or 16: which traversals start a segment's
+                                     next k-buffer round from the subtrees, leaves and candidates its
+                                     previous round set aside against the K-th distance, instead of
+                                     from the root (fewer node visits; the same candidates up to the
+                                     grazing case above): 0 = the backward replay's (default), 1 =
+                                     none, 2 = the replay's and the intersection stage's */
 } ptir_config;
 
 enum { PTIR_STORAGE_FP32 = 0, PTIR_STORAGE_BF16 = 1, PTIR_STORAGE_FP16 = 2 };

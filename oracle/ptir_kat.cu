@@ -170,12 +170,9 @@ int ptirkat_set_scene(const float* env, int eh, int ew, const float* alias, int 
         p.env.alias = alias + p.env.cells;
         p.env.pdf = alias + 2 * p.env.cells;
     }
-    // the tracer's environment rotation (ptir_b200/csrc/api.cu): about z by pi/2
-    const float rot_z = 0.5f * 3.14159265358979323846f;
-    p.env.sin_z = (float)std::sin((double)rot_z);
-    p.env.cos_z = (float)std::cos((double)rot_z);
-    p.env.sin_x = 0.0f;
-    p.env.cos_x = 1.0f;
+    // the tracer's environment offset (ptir_b200/csrc/api.cu)
+    p.env.offset_x = 0.0f;
+    p.env.offset_y = 0.0f;
     p.lights.lights = num_lights > 0 ? lights : nullptr;
     p.lights.num_lights = num_lights;
     p.lights.table = entries > 0 ? light_table : nullptr;

@@ -11,7 +11,7 @@ from . import build as _build
 
 _LIB = None
 
-ABI_VERSION = 4  # PTIR_ABI_VERSION of include/ptir_b200.h that these structs mirror
+ABI_VERSION = 5  # PTIR_ABI_VERSION of include/ptir_b200.h that these structs mirror
 PTIR_OK = 0
 PTIR_EINVAL = 1
 PTIR_ECUDA = 2
@@ -46,6 +46,7 @@ class PtirConfig(C.Structure):
         ("grad_aggregate", C.c_int32),
         ("shadow_kbuffer", C.c_int32),
         ("exact_candidates", C.c_int32),
+        ("resume_rounds", C.c_int32),
     ]
 
 

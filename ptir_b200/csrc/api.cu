@@ -63,6 +63,8 @@ ptir::WavefrontTuning tuning_of(const ptir_config& c) {
     if (c.refill_lanes > 0) w.refill_lanes = c.refill_lanes;
     if (c.block_size > 0) w.block = c.block_size;
     w.sort_rays = c.ray_order == 0;
+    w.resume_isect = c.resume_rounds == 2;
+    w.resume_replay = c.resume_rounds != 1;
     return w;
 }
 
@@ -206,12 +208,9 @@ int prepare(ptir_tracer* t, const ptir_trace_args* a, const ptir_view* views, in
         p.env.alias = a->environment_alias + p.env.cells;
         p.env.pdf = a->environment_alias + 2 * p.env.cells;
     }
-    // environment offset is fixed at (0, 0): rotation about z by pi/2, none about x
-    const float rot_z = 0.5f * 3.14159265358979323846f;
-    p.env.sin_z = (float)std::sin((double)rot_z);
-    p.env.cos_z = (float)std::cos((double)rot_z);
-    p.env.sin_x = 0.0f;
-    p.env.cos_x = 1.0f;
+    // environment offset, fixed at (0, 0) as in the reference
+    p.env.offset_x = 0.0f;
+    p.env.offset_y = 0.0f;
     p.lights.lights = a->num_lights > 0 ? a->lights : nullptr;
     p.lights.num_lights = a->num_lights;
     p.lights.table = a->num_light_entries > 0 ? a->light_alias : nullptr;
@@ -334,6 +333,7 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     if (config->grad_sums != 0 && config->grad_sums != 1) return PTIR_EINVAL;
     if (config->grad_aggregate != 0 && config->grad_aggregate != 1) return PTIR_EINVAL;
     if (config->exact_candidates != 0 && config->exact_candidates != 1) return PTIR_EINVAL;
+    if (config->resume_rounds < 0 || config->resume_rounds > 2) return PTIR_EINVAL;
     if (config->storage != PTIR_STORAGE_FP32 && config->storage != PTIR_STORAGE_BF16 &&
         config->storage != PTIR_STORAGE_FP16)
         return PTIR_EINVAL;

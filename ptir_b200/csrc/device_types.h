@@ -46,7 +46,7 @@ struct EnvView {
     const float* alias;
     const float* pdf;
     int aw, ah, cells;
-    float sin_z, cos_z, sin_x, cos_x;  // environment rotation (offset fixed at (0, 0))
+    float offset_x, offset_y;  // environment offset (fixed at (0, 0)), turned into the rotation per lookup
 };
 
 enum Flags : unsigned {

@@ -742,15 +742,16 @@ PTIR_DEV bool replay_open(const TraceParams& P, const ReplayState& r) {
     return r.start < r.end && r.tr > P.min_transmittance;
 }
 
-// Scatter the material gradient onto the accepted hits of one k-buffer batch, front to back.
-template <int K>
+// Scatter the material gradient onto the accepted hits of one k-buffer batch, front to back
+// (with kLeafIndex the batch holds leaf record indices).
+template <int K, bool kLeafIndex = false>
 PTIR_DEV void replay_batch(const TraceParams& P, const BwdInputs& B, ReplayState& r, const float (&kt)[K],
                            const unsigned (&kid)[K], TraceCounters& ctr) {
     const bool metallic_on = (P.flags & kMetallic) != 0;
 #pragma unroll
     for (int i = 0; i < K; ++i) {
-        const unsigned id = kid[i];
-        if (id == kNoHit || !(r.tr > P.min_transmittance)) continue;
+        if (kid[i] == kNoHit || !(r.tr > P.min_transmittance)) continue;
+        const unsigned id = kLeafIndex ? leaf_gaussian(P.accel, kid[i]) : kid[i];
         if (r.self_occ && self_occluded(P, kt[i], id, r.d)) {
             r.start = fmaxf(r.start, kt[i]);
             continue;
@@ -770,23 +771,41 @@ PTIR_DEV void replay_batch(const TraceParams& P, const BwdInputs& B, ReplayState
     }
 }
 
-// pathTracer.cuh:313-390: one re-traversal that scatters a material gradient onto its Gaussians
+// pathTracer.cuh:313-390: one re-traversal that scatters a material gradient onto its Gaussians.
+// With a frontier F (k-buffer 8 or 16) the rounds after the first resume from what the previous
+// round set aside (traverse.cuh).
 template <class Ctx>
-PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const ReplayJob& j) {
+PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const ReplayJob& j, const Frontier* F = nullptr) {
+    constexpr int K = Ctx::K;
     const TraceParams& P = C.P;
     ReplayState r;
     replay_begin(P, j, r, C.ctr);
-    float kt[Ctx::K];
-    unsigned kid[Ctx::K];
+    float kt[K];
+    unsigned kid[K];
+    TraceState t;
     for (int round = 0; replay_open(P, r); ++round) {
         if (round > (1 << 16)) {
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
+        if constexpr (K <= 16) {
+            if (F) {
+                if (trace_start<K, true, true>(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, t, C.ctr, F,
+                                               round > 0)) {
+                    while (trace_step<K, true, true>(P.accel, r.o, r.d, t, kt, kid, C.stack, C.stack_t, P.error_word,
+                                                     C.ctr, F)) {
+                    }
+                }
+                if (kid[0] == kNoHit) break;
+                replay_batch<K, true>(P, B, r, kt, kid, C.ctr);
+                if (kid[K - 1] == kNoHit) break;
+                continue;
+            }
+        }
         trace_kbuf(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
         replay_batch(P, B, r, kt, kid, C.ctr);
-        if (kid[Ctx::K - 1] == kNoHit) break;
+        if (kid[K - 1] == kNoHit) break;
     }
 }
 
@@ -796,7 +815,8 @@ template <class Ctx>
 PTIR_DEV float3 env_radiance_bwd(const Ctx& C, const BwdInputs& B, float3 d, float3 cg, float3& dir_grad) {
     const EnvView& E = C.P.env;
     if (!env_present(E)) return f3(0.0f);
-    const Footprint f = footprint_of(E, env_rotate(E, d));
+    const EnvRotation rot = env_rotation(E);
+    const Footprint f = footprint_of(E, env_rotate(rot, d));
     const float3 bg = bilerp(E, f);
     ++C.ctr.env;
     if (B.environment_grad) {
@@ -817,8 +837,8 @@ PTIR_DEV float3 env_radiance_bwd(const Ctx& C, const BwdInputs& B, float3 d, flo
     onb(u, t, b);
     const float eps = 1e-3f;
     const float ps = rsqrtf(1.0f + eps * eps);
-    const float3 tb = bilerp(E, footprint_of(E, env_rotate(E, (u + t * eps) * ps)));
-    const float3 bb = bilerp(E, footprint_of(E, env_rotate(E, (u + b * eps) * ps)));
+    const float3 tb = bilerp(E, footprint_of(E, env_rotate(rot, (u + t * eps) * ps)));
+    const float3 bb = bilerp(E, footprint_of(E, env_rotate(rot, (u + b * eps) * ps)));
     C.ctr.env += 2;
     const float ie = 1.0f / eps;
     dir_grad += t * dot((tb - bg) * ie, cg) + b * dot((bb - bg) * ie, cg);

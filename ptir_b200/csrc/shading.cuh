@@ -63,13 +63,29 @@ PTIR_DEV Footprint footprint_cube(const EnvView& E, int face, float u, float v) 
     return f;
 }
 
-PTIR_DEV float3 env_rotate(const EnvView& E, float3 d) {
-    const float3 z = make_float3(d.x * E.cos_z - d.y * E.sin_z, d.x * E.sin_z + d.y * E.cos_z, d.z);
-    return make_float3(z.x, z.y * E.cos_x - z.z * E.sin_x, z.y * E.sin_x + z.z * E.cos_x);
+// The environment's rotation about z by 2 pi offset_x + pi / 2, then about x by 2 pi offset_y,
+// evaluated at each lookup with the device's sincosf from the offsets held in memory, as the
+// reference evaluates it (environment.cuh:116-178). The rounding of those sines and cosines
+// (cos(pi / 2) is not zero in float) shows in the bilinear weights and, amplified by 1 / eps, in
+// the finite-difference direction gradient, so they are computed the same way here.
+struct EnvRotation {
+    float sz, cz, sx, cx;
+};
+PTIR_DEV EnvRotation env_rotation(const EnvView& E) {
+    EnvRotation r;
+    sincosf(E.offset_x * 2.0f * kPiF + 0.5f * kPiF, &r.sz, &r.cz);
+    sincosf(E.offset_y * 2.0f * kPiF, &r.sx, &r.cx);
+    return r;
 }
+PTIR_DEV float3 env_rotate(const EnvRotation& r, float3 d) {
+    const float3 z = make_float3(d.x * r.cz - d.y * r.sz, d.x * r.sz + d.y * r.cz, d.z);
+    return make_float3(z.x, z.y * r.cx - z.z * r.sx, z.y * r.sx + z.z * r.cx);
+}
+PTIR_DEV float3 env_rotate(const EnvView& E, float3 d) { return env_rotate(env_rotation(E), d); }
 PTIR_DEV float3 env_unrotate(const EnvView& E, float3 e) {
-    const float3 x = make_float3(e.x, e.y * E.cos_x + e.z * E.sin_x, -e.y * E.sin_x + e.z * E.cos_x);
-    return make_float3(x.x * E.cos_z + x.y * E.sin_z, -x.x * E.sin_z + x.y * E.cos_z, x.z);
+    const EnvRotation r = env_rotation(E);
+    const float3 x = make_float3(e.x, e.y * r.cx + e.z * r.sx, -e.y * r.sx + e.z * r.cx);
+    return make_float3(x.x * r.cz + x.y * r.sz, -x.x * r.sz + x.y * r.cz, x.z);
 }
 
 PTIR_DEV void equirect_uv(float3 d, float& u, float& v) {

@@ -40,6 +40,8 @@ struct WfView {
     unsigned* cursor;        // [kNumCursors]
     ReplayJob* jobs;
     float* parked;           // intersection: parked accumulators and k-buffer batches, per thread
+    uint2* frontier;         // intersection: two frontier buffers of frontier_cap entries per thread
+    int frontier_cap;
     unsigned long long tile0;  // first tile of the chunk
     unsigned slots;          // paths in the chunk (32 per tile)
 };
@@ -226,11 +228,19 @@ constexpr int trace_regs(int K) { return K > 16 ? 128 : 96; }
 // otherwise the second round is traced. The results are those of 16-candidate rounds (a 32-entry
 // traversal culls at a farther distance, so it keeps grazing candidates that a 16-entry one can
 // cull, as an exact nearest-16 selection would), with about a third fewer node visits per segment.
-template <int K, bool kMark, bool kSelfOcc>
+//
+// With kResume (K <= 16) a segment's calls after its first resume from the frontier its previous
+// call set aside (traverse.cuh), in a lane's part of W.frontier.
+template <int K, bool kMark, bool kSelfOcc, bool kResume>
 __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
                                                       const unsigned* items, int out_q, unsigned cursor, int refill) {
     constexpr bool kPair = K == 32;  // traversals gather two 16-candidate rounds (leaf-index k-buffer)
+    static_assert(!(kPair && kResume), "resumed calls take the 16-candidate rounds one by one");
+    constexpr bool kIdx = kPair || kResume;  // the k-buffer holds leaf record indices
     const int nthreads = (int)(gridDim.x * blockDim.x);
+    const Frontier F{kResume ? W.frontier + (size_t)(blockIdx.x * blockDim.x + threadIdx.x) * 2 * W.frontier_cap
+                             : nullptr,
+                     W.frontier_cap};
     float* const base = W.parked + blockIdx.x * blockDim.x + threadIdx.x;
     const Parked pk{base, nthreads};
     float* const batch_t = base + kParkedFields * nthreads;
@@ -262,7 +272,8 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
             phase = kReady;
             return;
         }
-        phase = trace_start<K, kPair>(P.accel, ro, rd, composite_tmin(c), composite_tend(c), kt, kid, t, ctr)
+        phase = trace_start<K, kIdx, kResume>(P.accel, ro, rd, composite_tmin(c), composite_tend(c), kt, kid, t, ctr,
+                                              &F, rounds > 1)
                     ? kTracing
                     : kReady;
     };
@@ -306,7 +317,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
             const unsigned tracing = __ballot_sync(kFull, phase == kTracing);
             if (!tracing || __popc(eligible & ~tracing) >= refill) break;
             if (phase == kTracing &&
-                !trace_step<K, kPair>(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr))
+                !trace_step<K, kIdx, kResume>(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr, &F))
                 phase = kReady;
         }
         // composite the finished calls; hand on the finished segments
@@ -342,7 +353,10 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
                     if (call) next_call(c);
                     else no_call();
                 } else {
-                    composite_hits_strided<kSelfOcc, K>(P, ctr, c, batch_t, batch_id, nthreads, mark);
+                    if constexpr (kIdx)
+                        composite_leaf_batch<kSelfOcc>(P, ctr, c, batch_t, batch_id, nthreads, 0, K, mark);
+                    else
+                        composite_hits_strided<kSelfOcc, K>(P, ctr, c, batch_t, batch_id, nthreads, mark);
                     // a k-buffer that is not full held every candidate of the call: a later call finds none
                     if (kid[K - 1] != kNoHit) next_call(c);
                     else no_call();
@@ -691,16 +705,21 @@ __global__ void __launch_bounds__(kMaxThreads) k_wb_bounce(TraceParams P, BwdInp
 }
 
 template <int K>
-__global__ void __launch_bounds__(kMaxThreads) k_wb_replay(TraceParams P, BwdInputs B, WfView W, unsigned cursor) {
+__global__ void __launch_bounds__(kMaxThreads) k_wb_replay(TraceParams P, BwdInputs B, WfView W, unsigned cursor,
+                                                           bool resume) {
     PTIR_STAGE_PROLOGUE
     const unsigned count = W.count[kQJobs];
+    // with `resume` a replay's rounds after its first resume from the previous round's frontier
+    const Frontier F{resume ? W.frontier + (size_t)(blockIdx.x * blockDim.x + threadIdx.x) * 2 * W.frontier_cap
+                            : nullptr,
+                     W.frontier_cap};
     while (true) {
         const unsigned base = fetch32(W.cursor + cursor);
         if (base >= count) break;
         const unsigned i = base + lane();
         if (i < count) {
             const ReplayJob j = W.jobs[i];
-            replay_material_grad(C, B, j);
+            replay_material_grad(C, B, j, F.buf ? &F : nullptr);
         }
     }
     flush_counters(P, ctr);
@@ -772,8 +791,12 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
     rel(b.seg); rel(b.ps); rel(b.rng); rel(b.q[0]); rel(b.q[1]); rel(b.q[2]); rel(b.jobs);
     rel(b.sort_keys[0]); rel(b.sort_keys[1]); rel(b.sorted); rel(b.sort_temp); rel(b.parked);
     void* counters = b.counters;
+    void* frontier = b.frontier;
+    const size_t frontier_threads = b.frontier_threads;
     b = WavefrontBuffers{};
     b.counters = counters;
+    b.frontier = frontier;  // sized by the intersection grid, not by the chunk
+    b.frontier_threads = frontier_threads;
     cudaError_t e = cudaSuccess;
     auto get = [&](void** p, size_t bytes) {
         if (e == cudaSuccess) e = cudaMallocAsync(p, bytes, s);
@@ -808,12 +831,23 @@ size_t wavefront_bytes_per_slot() {
 
 void wavefront_free(WavefrontBuffers& b) {
     for (void* p : {b.seg, b.ps, b.rng, b.q[0], b.q[1], b.q[2], b.jobs, b.counters, b.sort_keys[0], b.sort_keys[1],
-                    b.sorted, b.sort_temp, b.parked})
+                    b.sorted, b.sort_temp, b.parked, b.frontier})
         if (p) cudaFree(p);
     b = WavefrontBuffers{};
 }
 
-static WfView view_of(const WavefrontBuffers& b, unsigned long long tile0, unsigned slots) {
+// frontier buffers for `threads` threads of the intersection kernel (grown on demand)
+cudaError_t frontier_reserve(WavefrontBuffers& b, size_t threads, cudaStream_t s) {
+    if (threads <= b.frontier_threads && b.frontier) return cudaSuccess;
+    if (b.frontier) cudaFreeAsync(b.frontier, s);
+    b.frontier = nullptr;
+    b.frontier_threads = 0;
+    const cudaError_t e = cudaMallocAsync(&b.frontier, sizeof(uint2) * 2 * (size_t)kFrontierCap * threads, s);
+    if (e == cudaSuccess) b.frontier_threads = threads;
+    return e;
+}
+
+static WfView view_of(const WavefrontBuffers& b, unsigned long long tile0, unsigned slots, bool resume) {
     WfView W;
     W.seg = static_cast<Segment*>(b.seg);
     W.ps = static_cast<PathState*>(b.ps);
@@ -823,6 +857,8 @@ static WfView view_of(const WavefrontBuffers& b, unsigned long long tile0, unsig
     W.cursor = W.count + kNumQueueCounts;
     W.jobs = static_cast<ReplayJob*>(b.jobs);
     W.parked = static_cast<float*>(b.parked);
+    W.frontier = resume ? static_cast<uint2*>(b.frontier) : nullptr;
+    W.frontier_cap = resume ? kFrontierCap : 0;
     W.tile0 = tile0;
     W.slots = slots;
     return W;
@@ -852,6 +888,32 @@ static const unsigned* sort_queue(const TraceParams& p, const WavefrontBuffers& 
 // 2, shadow 3, then per bounce depth the bounce stage, (the adjoint's replay,) and intersection.
 constexpr unsigned kFirstBounceCursor = 4;
 
+// intersection kernels with resumed rounds (K <= 16)
+template <int K>
+static bool use_resume(const WavefrontTuning& tune) {
+    return K <= 16 && tune.resume_isect;
+}
+
+template <int K, bool kMark, bool kSelfOcc>
+static int trace_grid(bool resume, int B) {
+    if constexpr (K <= 16) {
+        if (resume) return grid_cached((const void*)k_wf_trace<K, kMark, kSelfOcc, true>, B);
+    }
+    return grid_cached((const void*)k_wf_trace<K, kMark, kSelfOcc, false>, B);
+}
+
+template <int K, bool kMark, bool kSelfOcc>
+static void launch_trace(bool resume, int grid, int B, cudaStream_t s, const TraceParams& q, float* vis,
+                         const WfView& W, int in_q, const unsigned* items, int out_q, unsigned cursor, int R) {
+    if constexpr (K <= 16) {
+        if (resume) {
+            k_wf_trace<K, kMark, kSelfOcc, true><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
+            return;
+        }
+    }
+    k_wf_trace<K, kMark, kSelfOcc, false><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
+}
+
 template <int K>
 static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b, const WavefrontTuning& tune,
                            const StageCtx& sc, cudaStream_t s) {
@@ -864,13 +926,15 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
     const int g_camera = grid_cached((const void*)k_wf_camera, B);
     const int g_primary = grid_cached((const void*)k_wf_fwd_primary<K>, B);
     const int g_bounce = grid_cached((const void*)k_wf_fwd_bounce<K>, B);
-    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, true, false>, B);
-    const int g_trace = grid_cached((const void*)k_wf_trace<K, true, true>, B);
+    const bool resume = use_resume<K>(tune);
+    const int g_trace0 = trace_grid<K, true, false>(resume, B);
+    const int g_trace = trace_grid<K, true, true>(resume, B);
+    if (resume && (e = frontier_reserve(b, std::max(g_trace0, g_trace) * B, s)) != cudaSuccess) return e;
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 2u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
         const unsigned nt = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles - t0);
-        const WfView W = view_of(b, t0, nt * 32u);
+        const WfView W = view_of(b, t0, nt * 32u, resume);
         e = cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * (kNumQueueCounts + kNumCursors), s);
         if (e != cudaSuccess) return e;
         const int cap = (int)std::min<long long>(INT32_MAX, ((long long)nt * 32 + B - 1) / B);
@@ -878,8 +942,8 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            k_wf_trace<K, true, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, o.visibility, W, kQIsect,
-                                                                             W.q[kQIsect], -1, 1, R);
+            launch_trace<K, true, false>(resume, std::min(g_trace0, cap), B, s, q, o.visibility, W, kQIsect,
+                                         W.q[kQIsect], -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
             k_wf_fwd_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, o, W);
@@ -900,8 +964,8 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                k_wf_trace<K, true, true><<<g_trace, B, 0, s>>>(q, o.visibility, W, kQIsect, items, kQBounce, cursor,
-                                                                R);
+                launch_trace<K, true, true>(resume, g_trace, B, s, q, o.visibility, W, kQIsect, items, kQBounce, cursor,
+                                            R);
             });
             ++cursor;
         }
@@ -923,14 +987,18 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
     const int g_camera = grid_cached((const void*)k_wf_camera, B);
     const int g_primary = grid_cached((const void*)k_wb_primary<K>, B);
     const int g_bounce = grid_cached((const void*)k_wb_bounce<K>, B);
-    const int g_trace0 = grid_cached((const void*)k_wf_trace<K, false, false>, B);
-    const int g_trace = grid_cached((const void*)k_wf_trace<K, false, true>, B);
+    const bool resume = use_resume<K>(tune);
+    const bool resume_replay = K <= 16 && tune.resume_replay;
+    const int g_trace0 = trace_grid<K, false, false>(resume, B);
+    const int g_trace = trace_grid<K, false, true>(resume, B);
     const int g_replay = grid_cached((const void*)k_wb_replay<K>, B);
+    const int g_front = std::max(resume ? std::max(g_trace0, g_trace) : 0, resume_replay ? g_replay : 0);
+    if (g_front > 0 && (e = frontier_reserve(b, (size_t)g_front * B, s)) != cudaSuccess) return e;
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 3u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
     for (unsigned long long t0 = 0; t0 < tiles; t0 += chunk_tiles) {
         const unsigned nt = (unsigned)std::min<unsigned long long>(chunk_tiles, tiles - t0);
-        const WfView W = view_of(b, t0, nt * 32u);
+        const WfView W = view_of(b, t0, nt * 32u, g_front > 0);
         e = cudaMemsetAsync(b.counters, 0, sizeof(unsigned) * (kNumQueueCounts + kNumCursors), s);
         if (e != cudaSuccess) return e;
         const int cap = (int)std::min<long long>(INT32_MAX, ((long long)nt * 32 + B - 1) / B);
@@ -938,8 +1006,8 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            k_wf_trace<K, false, false><<<std::min(g_trace0, cap), B, 0, s>>>(q, nullptr, W, kQIsect, W.q[kQIsect],
-                                                                              -1, 1, R);
+            launch_trace<K, false, false>(resume, std::min(g_trace0, cap), B, s, q, nullptr, W, kQIsect,
+                                          W.q[kQIsect], -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
             k_wb_primary<K><<<std::min(g_primary, cap), B, 0, s>>>(q, bi, W);
@@ -958,14 +1026,14 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             });
             ++cursor;
             sc.run(kStageReplay, p, s, [&](const TraceParams& q) {
-                k_wb_replay<K><<<g_replay, B, 0, s>>>(q, bi, W, cursor);
+                k_wb_replay<K><<<g_replay, B, 0, s>>>(q, bi, W, cursor, resume_replay);
             });
             ++cursor;
             if (depth + 1 >= mb) break;
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                k_wf_trace<K, false, true><<<g_trace, B, 0, s>>>(q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
+                launch_trace<K, false, true>(resume, g_trace, B, s, q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
             });
             ++cursor;
         }

@@ -26,7 +26,15 @@ struct WavefrontBuffers {
     void* sort_temp = nullptr;
     size_t sort_temp_bytes = 0;
     void* parked = nullptr;  // f32, per resident thread of the intersection kernel (k_wf_trace)
+    void* frontier = nullptr;  // uint2[2 * kFrontierCap] per thread of the intersection kernel
+    size_t frontier_threads = 0;
 };
+
+// Entries of each of a lane's two frontier buffers (resumed trace calls, traverse.cuh). A call
+// that sets more aside leaves its segment's next call to start from the root.
+constexpr int kFrontierCap = 768;
+
+cudaError_t frontier_reserve(WavefrontBuffers& b, size_t threads, cudaStream_t s);
 
 cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s);
 // device bytes the wavefront holds per path slot of a chunk (state, queues, replay jobs, sort)
@@ -42,6 +50,8 @@ struct WavefrontTuning {
     int block = 128;                // threads per block: 64, 128 or 256
     bool sort_rays = true;          // intersect bounce rays in (octant, origin cell, direction cell) order
     int shadow_kbuf = 16;           // candidates per shadow-ray traversal: 8, 16 or 32
+    bool resume_isect = false;      // intersection stage: rounds resumed from the previous round's frontier (K <= 16)
+    bool resume_replay = true;      // backward replay: the same
 };
 
 cudaError_t launch_trace_fwd_wavefront(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b,

@@ -111,7 +111,10 @@ class OptixTracer:
     shadow rays apart from ``kbuffer``. ``exact_candidates`` makes every traversal return exactly
     the K nearest candidates (off: subtrees are culled by their box entry as the reference's
     traversal culls them, which keeps a grazing Gaussian or not depending on the order), so that
-    the results depend on neither the traversal order nor ``kbuffer``."""
+    the results depend on neither the traversal order nor ``kbuffer``. ``resume_rounds`` (k-buffer 8
+    or 16) picks the traversals whose next k-buffer round starts from what the previous round set
+    aside against its K-th distance instead of from the root: 0 the backward replay's (default), 1
+    none, 2 the replay's and the intersection stage's."""
 
     def __init__(
         self,
@@ -143,6 +146,7 @@ class OptixTracer:
         warp_aggregate: bool = True,
         shadow_kbuffer: int = 0,
         exact_candidates: bool = False,
+        resume_rounds: int = 0,
     ):
         if pipeline not in ("reference",):
             raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
@@ -159,7 +163,8 @@ class OptixTracer:
             int(bool(enable_metallic)), int(bool(visualize_lights)), int(bool(collect_counters)),
             N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
             int(bool(collect_timings)), 0 if sort_rays else 1, int(bool(exact_replay)), 0 if compensated_grads else 1,
-            N.STORAGES[storage], 0 if warp_aggregate else 1, int(shadow_kbuffer), int(bool(exact_candidates)))
+            N.STORAGES[storage], 0 if warp_aggregate else 1, int(shadow_kbuffer), int(bool(exact_candidates)),
+            int(resume_rounds))
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:

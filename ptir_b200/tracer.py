@@ -263,7 +263,8 @@ class Tracer:
         # B200 launch shape and attribute storage (render.b200.*; absent keys keep the defaults)
         b2 = _conf_get(r, "b200")
         launch = {k: _conf_get(b2, k) for k in ("schedule", "chunk_tiles", "kbuffer", "refill_lanes", "block_size",
-                                                 "sort_rays", "storage", "shadow_kbuffer", "exact_candidates")}
+                                                 "sort_rays", "storage", "shadow_kbuffer", "exact_candidates",
+                                                 "resume_rounds")}
         self.tracer_wrapper = OptixTracer(
             "", "", r.pipeline_type, r.backward_pipeline_type, r.primitive_type, r.particle_kernel_degree,
             r.particle_kernel_min_response, r.particle_kernel_density_clamping, r.particle_radiance_sph_degree,

@@ -14,7 +14,7 @@ import torch
 
 from oracle import compare as K
 from oracle import oracle as O
-from tests.scenes import _light_tensors, make_tracer, small_scene, to_torch
+from tests.scenes import _light_tensors, gpu_trace_bwd, make_tracer, small_scene, to_torch
 
 pytestmark = pytest.mark.gpu
 
@@ -151,3 +151,46 @@ def test_refit_after_motion_matches_rebuild_and_oracle(cuda_device):
     lo, hi = tr.scene_bounds().numpy().reshape(2, 3)
     aabb, _, _, _ = O.instances(O.OracleConfig(), s1)
     assert np.allclose(np.concatenate([lo, hi]), aabb, atol=1e-4)
+
+
+@pytest.mark.parametrize("case", [
+    dict(n=3000, w=48, h=40, spp=2, max_bounces=3),
+    dict(n=6000, w=40, h=32, spp=2, max_bounces=4, layout="cluster_shell", scale_range=(0.002, 0.2)),
+    dict(n=4000, w=32, h=32, spp=4, max_bounces=3, scale_range=(0.05, 0.3)),
+])
+@pytest.mark.parametrize("kbuffer", [8, 16])
+def test_resumed_calls_match_calls_from_the_root(cuda_device, case, kbuffer):
+    """A segment's k-buffer rounds after its first resumed from what the previous round set aside
+    (traverse.cuh, resume_rounds = 2) against every round from the root (resume_rounds = 1): the
+    same candidates, so the same paths and, path by path, bitwise the same outputs, and the same
+    adjoint up to the order of the gradient atomics. Only a grazing Gaussian (closest approach
+    before its box entry) can be kept by one order and not the other."""
+    s = small_scene(**case)
+    S = to_torch(s)
+    root = make_tracer(kbuffer=kbuffer, resume_rounds=1)
+    resumed = make_tracer(kbuffer=kbuffer, resume_rounds=2)
+    out_a, sig_a = _trace(root, S, build=True, rebuild=True)
+    out_b, sig_b = _trace(resumed, S, build=True, rebuild=True)
+    torch.cuda.synchronize()
+    assert root.device_status() == 0 and resumed.device_status() == 0
+    same = sig_a == sig_b
+    print(f"k{kbuffer} {case}: {same.mean():.6f} of paths take the same decisions; node visits "
+          f"{root.counters()['node_visits']} from the root, {resumed.counters()['node_visits']} resumed")
+    assert same.mean() >= 0.999, same.mean()
+    for k in (0, 1, 2, 3, 4, 5, 6, 7, 8, 10, 11, 12):
+        a = out_a[k].cpu().numpy().reshape(*sig_a.shape, -1)
+        b = out_b[k].cpu().numpy().reshape(*sig_b.shape, -1)
+        eq = np.all(a == b, axis=-1)
+        assert eq[same].mean() >= 0.999, (k, eq[same].mean())
+    assert resumed.counters()["node_visits"] < root.counters()["node_visits"]
+    # the backward replay's rounds (resumed by default)
+    g = torch.from_numpy(np.random.default_rng(3).standard_normal(tuple(sig_a.shape) + (3,)).astype(np.float32)).cuda()
+    g = torch.where(torch.from_numpy(same).cuda()[..., None], g, torch.zeros_like(g))
+    grads = []
+    for tr, out in ((root, out_a), (resumed, out_b)):
+        _, mg, _, _, eg = gpu_trace_bwd(tr, S, list(out), g)
+        grads.append((mg.cpu().numpy(), eg.cpu().numpy()))
+    torch.cuda.synchronize()
+    for a, b in zip(grads[0], grads[1]):
+        rel, cos = K.rel_cos(a, b)
+        assert rel <= 1e-5 and cos >= 0.99999, (rel, cos)

@@ -177,19 +177,25 @@ def test_sh_indirect_mode(cuda_device, schedule):
     dict(n=5000, w=64, h=48, spp=1, max_bounces=3, scale_range=(0.005, 0.05)),
 ])
 def test_paths_with_the_oracles_decisions_match_it(cuda_device, case):
-    """Split by path decision signatures (oracle/compare.py): the paths on which the float32 GPU
-    tracer takes every discrete branch as the FP64 oracle does are at least 99 % of all, and on
-    >= 99.8 % of them every output is within 1e-3 + 1e-3 |oracle| (the oracle's own FP32 build
-    does no better: float32 keeps about two digits of the reference's GGX distribution near the
-    specular peak at the clamped roughness).
-    The adjoint over those paths (the incoming pbr gradient zeroed on the others) matches the
-    oracle's to relative L2 <= 1e-3 and cosine >= 0.999 for the material and environment
-    gradients."""
+    """Split by path decision signatures (oracle/compare.py), with the oracle's own FP32 build as
+    the measure of what float32 can do on the same estimator and sample sequences:
+
+    - the GPU takes another discrete branch than FP64 on at most 0.2 % of the paths, or twice as
+      many as the FP32 build does;
+    - on the paths where the GPU, the FP32 build and FP64 take the same branches, every output is
+      within relative L2 1e-3 of FP64 (or three times the FP32 build's own distance), and no fewer
+      samples are within 1e-3 + 1e-3 |FP64| than the FP32 build's less 0.2 %;
+    - the adjoint over those paths (the incoming pbr gradient zeroed on the others): the albedo
+      gradient within relative L2 1e-3 and cosine 0.999 of FP64; the environment gradient and the
+      roughness gradient (whose reference term is a finite difference over 1e-3 of float
+      evaluations, material.cuh:362-375) within 1e-3 or three times the FP32 build's own
+      distance."""
     from oracle import compare as K
 
     s = small_scene(**case)
     cfg = O.OracleConfig()
     ref, _, _ = O.trace(cfg, s, "f64")
+    r32, _, _ = O.trace(cfg, s, "f32")
     tr = make_tracer()
     S = to_torch(s)
     zhw = s["ray_ori"].shape[:3]
@@ -200,24 +206,34 @@ def test_paths_with_the_oracles_decisions_match_it(cuda_device, case):
                    S["sph_degree"], S["min_transmittance"], S["max_bounces"], path_signature=sig_t)
     out = _gpu_outputs(res)
     sig = sig_t.cpu().numpy().view(np.uint32)
-    agree = sig == ref["path_sig"]
-    assert agree.mean() >= 0.99, agree.mean()
+    flipped, flipped32 = float((sig != ref["path_sig"]).mean()), float((r32["path_sig"] != ref["path_sig"]).mean())
+    assert flipped <= max(0.002, 2.0 * flipped32), (flipped, flipped32)
+    agree = (sig == ref["path_sig"]) & (r32["path_sig"] == ref["path_sig"])
     for k in KEYS:
-        ok = K.within(out[k].reshape(*zhw, -1), ref[k].reshape(*zhw, -1))
-        assert ok[agree].mean() >= 0.998, (k, float(ok[agree].mean()))
+        a, b, c = (x[k].reshape(*zhw, -1) for x in (out, ref, r32))
+        ok, ok32 = K.within(a, b), K.within(c, b)
+        rel, rel32 = K.rel_cos(a[agree], b[agree])[0], K.rel_cos(c[agree], b[agree])[0]
+        assert rel <= max(1e-3, 3 * rel32), (k, rel, rel32)
+        assert ok[agree].mean() >= ok32[agree].mean() - 0.002, (k, float(ok[agree].mean()), float(ok32[agree].mean()))
     # adjoint over the agreeing paths
     rng = np.random.default_rng(5)
     g = rng.standard_normal(zhw + (3,)).astype(np.float32)
-    g_m = K.masked_grad(g, sig, ref["path_sig"])
+    g_m = np.where(agree[..., None], g, 0.0).astype(np.float32)
     mg_ref, eg_ref, _ = O.trace_bwd(cfg, s, ref, dict(pbr=g_m), "f64")
+    mg32, eg32, _ = O.trace_bwd(cfg, s, r32, dict(pbr=g_m), "f32")
     fwd = list(res)
     fwd[10] = torch.from_numpy(ref["pbr"]).cuda()
     fwd[11] = torch.from_numpy(ref["light"]).cuda()
     _, mg, _, _, eg = gpu_trace_bwd(tr, S, fwd, torch.from_numpy(g_m).cuda())
-    rep = K.grad_report(mg.cpu().numpy(), eg.cpu().numpy(), mg_ref, eg_ref)
-    assert rep["material_rel_l2"] <= 1e-3 and rep["material_cos"] >= 0.999, rep
-    assert rep["env_rel_l2"] <= 1e-3 and rep["env_cos"] >= 0.999, rep
-
+    mg, eg = mg.cpu().numpy(), eg.cpu().numpy()
+    rel, cos = K.rel_cos(mg[:, :3], mg_ref[:, :3])
+    assert rel <= 1e-3 and cos >= 0.999, ("albedo", rel, cos)
+    rel, cos = K.rel_cos(eg[..., :3], eg_ref[..., :3])
+    rel32 = K.rel_cos(eg32[..., :3], eg_ref[..., :3])[0]
+    assert rel <= max(1e-3, 3.0 * rel32) and cos >= 0.999, ("environment", rel, rel32, cos)
+    rel, cos = K.rel_cos(mg[:, 3], mg_ref[:, 3])
+    rel32 = K.rel_cos(mg32[:, 3], mg_ref[:, 3])[0]
+    assert rel <= max(1e-3, 3.0 * rel32) and cos >= 0.999, ("roughness", rel, rel32, cos)
 
 
 def test_strided_per_sample_inputs_match_contiguous(cuda_device):
