@@ -65,6 +65,7 @@ ptir::WavefrontTuning tuning_of(const ptir_config& c) {
     w.sort_rays = c.ray_order == 0;
     w.resume_isect = c.resume_rounds == 2;
     w.resume_replay = c.resume_rounds != 1;
+    w.exact_candidates = c.exact_candidates != 0;
     return w;
 }
 

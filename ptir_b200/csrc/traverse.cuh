@@ -142,13 +142,18 @@ PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, floa
                                   r2.x * o.x + r2.y * o.y + r2.z * o.z + r2.w);
     const float3 dd = make_float3(r0.x * d.x + r0.y * d.y + r0.z * d.z, r1.x * d.x + r1.y * d.y + r1.z * d.z,
                                   r2.x * d.x + r2.y * d.y + r2.z * d.z);
-    float ts;
-    if (!instance_hit(od, dd, tmin, fminf(tend, cut), ts)) return false;
-    // object-space unit box within [tmin, tend]
+    // the three conditions of a candidate, cheapest rejection first: the closest approach's
+    // interval, the object-space unit box within [tmin, tend] (which rejects most of the rest), then
+    // the perpendicular distance of instance_hit (almost never the deciding one)
+    const float den = 1.0f / dot(dd, dd);
+    const float ts = -dot(od, dd) * den;
+    if (!(ts > tmin && ts < fminf(tend, cut))) return false;
     const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float b0, b1;
     slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
     if (fmaxf(b0, tmin) > fminf(b1, tend)) return false;
+    const float3 c = cross(normalize_or_keep(dd), od);
+    if (!(dot(c, c) * den < 9.0f)) return false;
     ts_out = ts;
     id_out = __float_as_uint(__ldg(&rec[3].x));
     return true;
@@ -244,12 +249,12 @@ PTIR_DEV int leaf_candidate3(const AccelView& A, int p, float3 o, float3 d, floa
     if (!(ts > tmin && ts < tend)) return 0;
     ts_out = ts;
     if (!(ts < cut)) return 2;
-    const float3 c = cross(normalize_or_keep(dd), od);
-    if (!(dot(c, c) * den < 9.0f)) return 0;
     const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float b0, b1;
     slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
     if (fmaxf(b0, tmin) > fminf(b1, tend)) return 0;
+    const float3 c = cross(normalize_or_keep(dd), od);
+    if (!(dot(c, c) * den < 9.0f)) return 0;
     id_out = __float_as_uint(__ldg(&rec[3].x));
     return 1;
 }
@@ -331,8 +336,10 @@ struct NodeVisit {
 };
 
 // Box tests of the node t.node. Returns the mask of leaf children to test. With kResume the
-// children whose box the ray crosses past the K-th distance are set aside in F.
-template <int K, bool kResume = false>
+// children whose box the ray crosses past the K-th distance are set aside in F. Without kSlack
+// the cull slack (exact candidates) is not applied: a kernel built so holds neither its registers
+// nor the kmax load.
+template <int K, bool kResume = false, bool kSlack = true>
 PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const float (&kt)[K], NodeVisit& v,
                              TraceCounters& ctr, const Frontier* F = nullptr) {
     const float3 inv = t.inv;
@@ -346,9 +353,11 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const 
     const float4 fx = __ldg(nd + (3 - rx)), fy = __ldg(nd + (5 - ry)), fz = __ldg(nd + (7 - rz));
     const float4 cc = __ldg(nd + 6);
     float sl[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-    if (t.slack > 0.0f) {
-        const float4 km = __ldg(nd + 7);
-        sl[0] = km.x * t.slack; sl[1] = km.y * t.slack; sl[2] = km.z * t.slack; sl[3] = km.w * t.slack;
+    if constexpr (kSlack) {
+        if (t.slack > 0.0f) {
+            const float4 km = __ldg(nd + 7);
+            sl[0] = km.x * t.slack; sl[1] = km.y * t.slack; sl[2] = km.z * t.slack; sl[3] = km.w * t.slack;
+        }
     }
     const float nxa[4] = {nx.x, nx.y, nx.z, nx.w}, nya[4] = {ny.x, ny.y, ny.z, ny.w};
     const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fxa[4] = {fx.x, fx.y, fx.z, fx.w};
@@ -369,7 +378,7 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const 
                               fmaxf(fmaf(nza[k], inv.z, -oi.z), tmin));
         const float b = min3f(fmaf(fxa[k], inv.x, -oi.x), fmaf(fya[k], inv.y, -oi.y),
                               fminf(fmaf(fza[k], inv.z, -oi.z), tend));
-        v.t0[k] = a - sl[k];
+        v.t0[k] = kSlack ? a - sl[k] : a;
         // nearer middle of the clipped interval first: boxes that contain the origin all
         // enter at tmin, their extent along the ray tells them apart
         v.key[k] = a + b;
@@ -458,7 +467,7 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
 // One 4-wide node visit of a trace call with its leaf tests in the lane (with kResume, t.node < 0
 // is a leaf set aside by the previous call, tested instead). Returns false when the call is
 // complete.
-template <int K, bool kLeafIndex = false, bool kResume = false, class Ids>
+template <int K, bool kLeafIndex = false, bool kResume = false, bool kSlack = true, class Ids>
 PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid, int* stack,
                          float* stack_t, unsigned* err, TraceCounters& ctr, const Frontier* F = nullptr) {
     NodeVisit v;
@@ -470,7 +479,7 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
         v.hits = 0;
         leaves = 0;
     } else {
-        leaves = visit_node<K, kResume>(A, o, t, kt, v, ctr, F);
+        leaves = visit_node<K, kResume, kSlack>(A, o, t, kt, v, ctr, F);
     }
     // leaf children: one test call site, looping over the mask
     while (leaves) {

@@ -230,12 +230,14 @@ constexpr int trace_regs(int K) { return K > 16 ? 128 : 96; }
 // cull, as an exact nearest-16 selection would), with about a third fewer node visits per segment.
 //
 // With kResume (K <= 16) a segment's calls after its first resume from the frontier its previous
-// call set aside (traverse.cuh), in a lane's part of W.frontier.
-template <int K, bool kMark, bool kSelfOcc, bool kResume>
+// call set aside (traverse.cuh), in a lane's part of W.frontier. kSlack builds the kernel that
+// applies the exact-candidate cull slack (only tracers with exact_candidates launch it).
+template <int K, bool kMark, bool kSelfOcc, bool kResume, bool kSlack>
 __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis, WfView W, int in_q,
                                                       const unsigned* items, int out_q, unsigned cursor, int refill) {
     constexpr bool kPair = K == 32;  // traversals gather two 16-candidate rounds (leaf-index k-buffer)
     static_assert(!(kPair && kResume), "resumed calls take the 16-candidate rounds one by one");
+    static_assert(!(kSlack && kResume), "the exact-candidate slack is applied by the rounds from the root");
     constexpr bool kIdx = kPair || kResume;  // the k-buffer holds leaf record indices
     const int nthreads = (int)(gridDim.x * blockDim.x);
     const Frontier F{kResume ? W.frontier + (size_t)(blockIdx.x * blockDim.x + threadIdx.x) * 2 * W.frontier_cap
@@ -317,7 +319,8 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
             const unsigned tracing = __ballot_sync(kFull, phase == kTracing);
             if (!tracing || __popc(eligible & ~tracing) >= refill) break;
             if (phase == kTracing &&
-                !trace_step<K, kIdx, kResume>(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr, &F))
+                !trace_step<K, kIdx, kResume, kSlack>(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr,
+                                                      &F))
                 phase = kReady;
         }
         // composite the finished calls; hand on the finished segments
@@ -891,27 +894,37 @@ constexpr unsigned kFirstBounceCursor = 4;
 // intersection kernels with resumed rounds (K <= 16)
 template <int K>
 static bool use_resume(const WavefrontTuning& tune) {
-    return K <= 16 && tune.resume_isect;
+    return K <= 16 && tune.resume_isect && !tune.exact_candidates;
 }
 
+// the intersection kernel of a launch: resumed rounds, the exact-candidate slack, or neither
 template <int K, bool kMark, bool kSelfOcc>
-static int trace_grid(bool resume, int B) {
+static const void* trace_kernel(bool resume, bool slack) {
     if constexpr (K <= 16) {
-        if (resume) return grid_cached((const void*)k_wf_trace<K, kMark, kSelfOcc, true>, B);
+        if (resume) return (const void*)k_wf_trace<K, kMark, kSelfOcc, true, false>;
     }
-    return grid_cached((const void*)k_wf_trace<K, kMark, kSelfOcc, false>, B);
+    if (slack) return (const void*)k_wf_trace<K, kMark, kSelfOcc, false, true>;
+    return (const void*)k_wf_trace<K, kMark, kSelfOcc, false, false>;
 }
 
 template <int K, bool kMark, bool kSelfOcc>
-static void launch_trace(bool resume, int grid, int B, cudaStream_t s, const TraceParams& q, float* vis,
+static int trace_grid(bool resume, bool slack, int B) {
+    return grid_cached(trace_kernel<K, kMark, kSelfOcc>(resume, slack), B);
+}
+
+template <int K, bool kMark, bool kSelfOcc>
+static void launch_trace(bool resume, bool slack, int grid, int B, cudaStream_t s, const TraceParams& q, float* vis,
                          const WfView& W, int in_q, const unsigned* items, int out_q, unsigned cursor, int R) {
     if constexpr (K <= 16) {
         if (resume) {
-            k_wf_trace<K, kMark, kSelfOcc, true><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
+            k_wf_trace<K, kMark, kSelfOcc, true, false><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
             return;
         }
     }
-    k_wf_trace<K, kMark, kSelfOcc, false><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
+    if (slack)
+        k_wf_trace<K, kMark, kSelfOcc, false, true><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
+    else
+        k_wf_trace<K, kMark, kSelfOcc, false, false><<<grid, B, 0, s>>>(q, vis, W, in_q, items, out_q, cursor, R);
 }
 
 template <int K>
@@ -926,9 +939,9 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
     const int g_camera = grid_cached((const void*)k_wf_camera, B);
     const int g_primary = grid_cached((const void*)k_wf_fwd_primary<K>, B);
     const int g_bounce = grid_cached((const void*)k_wf_fwd_bounce<K>, B);
-    const bool resume = use_resume<K>(tune);
-    const int g_trace0 = trace_grid<K, true, false>(resume, B);
-    const int g_trace = trace_grid<K, true, true>(resume, B);
+    const bool resume = use_resume<K>(tune), slack = tune.exact_candidates;
+    const int g_trace0 = trace_grid<K, true, false>(resume, slack, B);
+    const int g_trace = trace_grid<K, true, true>(resume, slack, B);
     if (resume && (e = frontier_reserve(b, std::max(g_trace0, g_trace) * B, s)) != cudaSuccess) return e;
     const unsigned mb = p.render_opts ? std::min(p.max_bounces, 2u) : p.max_bounces;
     if (kFirstBounceCursor + 2u * mb > (unsigned)kNumCursors) return cudaErrorInvalidValue;
@@ -942,7 +955,7 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            launch_trace<K, true, false>(resume, std::min(g_trace0, cap), B, s, q, o.visibility, W, kQIsect,
+            launch_trace<K, true, false>(resume, slack, std::min(g_trace0, cap), B, s, q, o.visibility, W, kQIsect,
                                          W.q[kQIsect], -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
@@ -964,8 +977,8 @@ static cudaError_t run_fwd(const TraceParams& p, const FwdOutputs& o, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                launch_trace<K, true, true>(resume, g_trace, B, s, q, o.visibility, W, kQIsect, items, kQBounce, cursor,
-                                            R);
+                launch_trace<K, true, true>(resume, slack, g_trace, B, s, q, o.visibility, W, kQIsect, items, kQBounce,
+                                            cursor, R);
             });
             ++cursor;
         }
@@ -987,10 +1000,10 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
     const int g_camera = grid_cached((const void*)k_wf_camera, B);
     const int g_primary = grid_cached((const void*)k_wb_primary<K>, B);
     const int g_bounce = grid_cached((const void*)k_wb_bounce<K>, B);
-    const bool resume = use_resume<K>(tune);
+    const bool resume = use_resume<K>(tune), slack = tune.exact_candidates;
     const bool resume_replay = K <= 16 && tune.resume_replay;
-    const int g_trace0 = trace_grid<K, false, false>(resume, B);
-    const int g_trace = trace_grid<K, false, true>(resume, B);
+    const int g_trace0 = trace_grid<K, false, false>(resume, slack, B);
+    const int g_trace = trace_grid<K, false, true>(resume, slack, B);
     const int g_replay = grid_cached((const void*)k_wb_replay<K>, B);
     const int g_front = std::max(resume ? std::max(g_trace0, g_trace) : 0, resume_replay ? g_replay : 0);
     if (g_front > 0 && (e = frontier_reserve(b, (size_t)g_front * B, s)) != cudaSuccess) return e;
@@ -1006,7 +1019,7 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             k_wf_camera<<<std::min(g_camera, cap), B, 0, s>>>(q, W);
         });
         sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-            launch_trace<K, false, false>(resume, std::min(g_trace0, cap), B, s, q, nullptr, W, kQIsect,
+            launch_trace<K, false, false>(resume, slack, std::min(g_trace0, cap), B, s, q, nullptr, W, kQIsect,
                                           W.q[kQIsect], -1, 1, R);
         });
         sc.run(kStageShading, p, s, [&](const TraceParams& q) {
@@ -1033,7 +1046,8 @@ static cudaError_t run_bwd(const TraceParams& p, const BwdInputs& bi, WavefrontB
             cudaMemsetAsync(W.count + kQBounce, 0, sizeof(unsigned), s);
             const unsigned* items = sort_queue(p, b, W, tune, sc, s);
             sc.run(kStageIntersect, p, s, [&](const TraceParams& q) {
-                launch_trace<K, false, true>(resume, g_trace, B, s, q, nullptr, W, kQIsect, items, kQBounce, cursor, R);
+                launch_trace<K, false, true>(resume, slack, g_trace, B, s, q, nullptr, W, kQIsect, items, kQBounce,
+                                             cursor, R);
             });
             ++cursor;
         }

@@ -52,6 +52,7 @@ struct WavefrontTuning {
     int shadow_kbuf = 16;           // candidates per shadow-ray traversal: 8, 16 or 32
     bool resume_isect = false;      // intersection stage: rounds resumed from the previous round's frontier (K <= 16)
     bool resume_replay = true;      // backward replay: the same
+    bool exact_candidates = false;  // the intersection kernel with the exact-candidate cull slack
 };
 
 cudaError_t launch_trace_fwd_wavefront(const TraceParams& p, const FwdOutputs& o, WavefrontBuffers& b,
