@@ -216,9 +216,8 @@ def _clock_summary(lines: list):
 STAGES = ("intersect", "shadow", "replay", "shading", "megakernel", "sort")
 KERNEL_OF_STAGE = {"intersect": "k_wf_trace", "shadow": "k_wf_shadow", "replay": "k_wb_replay",
                    "shading": "k_wf_camera/primary/bounce", "megakernel": "k_trace_fwd/k_trace_bwd",
-                   "sort": "k_wf_sort_keys + CUB radix sort"}
-ACCEL_KERNELS_PER_BUILD = 9  # k_prep, k_bounds_partial, k_bounds_final, k_morton, k_hierarchy, k_even_depth,
-#                              k_gather, k_refit, k_emit4 (plus CUB's radix-sort and scan kernels)
+                   "sort": "k_wf_sort_keys + radix sort"}
+ACCEL_KERNELS_PER_BUILD = 6  # the step's refit: k_prep, k_bounds_partial, k_bounds_final, k_gather, k_refit, k_emit4
 
 
 def stage_bytes(stage: str, c: dict, rec: dict) -> float:

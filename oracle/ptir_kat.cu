@@ -1,12 +1,14 @@
 // TEST INFRASTRUCTURE ONLY. The tracer's own device functions (ptir_b200/csrc) behind the same
 // known-answer entry points as the reference's kernels of oracle/ref_device_kat.cu: one thread per
 // case, inputs [n, IN] and outputs [n, OUT] floats in the same layouts, so that
-// tests/test_gpu_device_kat.py can run both on the cases of tests/golden/device_kat.npz. Built by
-// `make -C oracle` with the library's own nvcc flags.
+// tests/test_gpu_device_kat.py can run both on the cases of tests/golden/device_kat.npz. Also the
+// tracer's radix sort on device buffers (tests/test_gpu_sort.py). Built by `make -C oracle` with
+// the library's own nvcc flags.
 #include <cmath>
 #include <cstring>
 
 #include "../ptir_b200/csrc/path.cuh"
+#include "../ptir_b200/csrc/radix_sort.cuh"
 
 namespace {
 
@@ -233,6 +235,25 @@ int ptirkat_light_sample(int n, const float* in, float* out) {
 int ptirkat_light_pdf(int n, const float* in, float* out) {
     k_light_pdf<<<blocks(n), 128>>>(n, in, out, g_params);
     return finish();
+}
+
+// the tracer's radix sort of device buffers (keys of 32 or 64 bits, 32-bit values) by bits
+// [begin_bit, end_bit); 0 on success
+int ptirkat_radix_sort(int key_bytes, const void* keys_in, void* keys_out, const unsigned* vals_in, unsigned* vals_out,
+                       long long n, int begin_bit, int end_bit) {
+    const size_t bytes = key_bytes == 8 ? radix_sort_temp_bytes<unsigned long long>(n) : radix_sort_temp_bytes<unsigned>(n);
+    void* temp = nullptr;
+    if (bytes && cudaMalloc(&temp, bytes) != cudaSuccess) return 1;
+    cudaError_t e = key_bytes == 8
+                        ? radix_sort_pairs<unsigned long long>(temp, bytes, static_cast<const unsigned long long*>(keys_in),
+                                                               static_cast<unsigned long long*>(keys_out), vals_in, vals_out, n,
+                                                               begin_bit, end_bit, 0)
+                        : radix_sort_pairs<unsigned>(temp, bytes, static_cast<const unsigned*>(keys_in),
+                                                     static_cast<unsigned*>(keys_out), vals_in, vals_out, n, begin_bit,
+                                                     end_bit, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (temp) cudaFree(temp);
+    return e == cudaSuccess ? 0 : 1;
 }
 
 }  // extern "C"

@@ -1,7 +1,7 @@
 """Build recipe of ``libptir_b200.so`` (nvcc, sm_100a, in-tree).
 
 ``python -m ptir_b200.build`` compiles every CUDA source of ``ptir_b200/csrc`` into one shared
-library next to this file. Only nvcc and the CUDA toolkit headers (CUB) are needed; no GPU.
+library next to this file. Only nvcc and the CUDA toolkit headers are needed; no GPU.
 """
 from __future__ import annotations
 

@@ -5,20 +5,19 @@
 //                (the instance transform of threedgptir_tracer/src/particlePrimitives.cu:543-610)
 //   2. bounds    scene AABB = union of the instance AABBs (two-pass reduction)
 //   3. morton    60-bit extended Morton key: AABB centre and size
-//   4. sort      key/id radix sort (CUB)
+//   4. sort      key/id radix sort (radix_sort.cuh: stable LSD, 8-bit digits)
 //   5. gather    leaf records in key order
 //   6. hierarchy internal nodes from the sorted keys (ties broken by position)
 //   7. refit     bottom-up child boxes with arrival counters
 //   8. collapse  4-wide nodes, greedy by surface area (rebuild only)
 //   9. emit      the 4-wide node records the traversal reads
 // A refit (rebuild == false, same n) redoes 1, 2, 5, 7 and 9 in the stored leaf order and topology.
-#include <cub/device/device_radix_sort.cuh>
-
 #include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
 
+#include "radix_sort.cuh"
 #include "../../include/ptir_b200.h"
 #include "accel.h"
 #include "storage.cuh"
@@ -452,16 +451,15 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
     if (!refit) {
         k_morton<<<blocks, T, 0, s>>>(n, st.box, st.bounds, st.keys[0], st.ids[0]);
         PTIR_TRY(cudaGetLastError());
-        size_t need = 0;
-        PTIR_TRY(cub::DeviceRadixSort::SortPairs(nullptr, need, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, kKeyBits, s));
+        const size_t need = radix_sort_temp_bytes<unsigned long long>(n);
         if (need > st.sort_temp_bytes) {
             if (st.sort_temp) PTIR_TRY(cudaFreeAsync(st.sort_temp, s));
             st.sort_temp = nullptr;
             PTIR_TRY(cudaMallocAsync(&st.sort_temp, need, s));
             st.sort_temp_bytes = need;
         }
-        size_t have = st.sort_temp_bytes;
-        PTIR_TRY(cub::DeviceRadixSort::SortPairs(st.sort_temp, have, st.keys[0], st.keys[1], st.ids[0], st.ids[1], n, 0, kKeyBits, s));
+        PTIR_TRY(radix_sort_pairs<unsigned long long>(st.sort_temp, st.sort_temp_bytes, st.keys[0], st.keys[1], st.ids[0],
+                                                      st.ids[1], n, 0, kKeyBits, s));
         if (n > 1) {
             const unsigned iblocks = (unsigned)((n - 1 + T - 1) / T);
             k_hierarchy<<<iblocks, T, 0, s>>>(n, st.keys[1], st.nodes, st.parent);

@@ -14,7 +14,6 @@
 // HBM between stages; queues are appended with one atomic per warp (ballot + popc). The
 // intersect stage refills lanes one by one (k_wf_trace). The per-path order of random draws is
 // the megakernel's, so both schedules produce the same paths.
-#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cstdint>
@@ -22,6 +21,7 @@
 #include <mutex>
 #include <utility>
 
+#include "radix_sort.cuh"
 #include "path.cuh"
 #include "wavefront.h"
 
@@ -815,19 +815,16 @@ cudaError_t wavefront_reserve(WavefrontBuffers& b, size_t slots, cudaStream_t s)
     get(&b.sorted, sizeof(unsigned) * slots);
     get(&b.parked, sizeof(float) * parked_floats());
     if (e == cudaSuccess) {
-        size_t bytes = 0;
-        e = cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned*)nullptr, (unsigned*)nullptr,
-                                            (const unsigned*)nullptr, (unsigned*)nullptr, (int)slots, 0, kSortKeyBits, s);
-        b.sort_temp_bytes = bytes;
-        get(&b.sort_temp, bytes);
+        b.sort_temp_bytes = radix_sort_temp_bytes<unsigned>((long long)slots);
+        get(&b.sort_temp, b.sort_temp_bytes);
     }
     if (e == cudaSuccess) b.slots = slots;
     return e;
 }
 
 size_t wavefront_bytes_per_slot() {
-    // path state, RNG, three queues, two replay jobs, two sort keys + the sorted queue, and CUB's
-    // double-buffered radix-sort temporary (about two key / value pairs)
+    // path state, RNG, three queues, two replay jobs, two sort keys + the sorted queue, and the
+    // radix sort's scratch (a key / value pair per slot and its digit counts, rounded up)
     return sizeof(Segment) + sizeof(PathState) + sizeof(unsigned long long) + 3 * sizeof(unsigned) +
            2 * sizeof(ReplayJob) + 3 * sizeof(unsigned) + 4 * sizeof(unsigned);
 }
@@ -880,9 +877,8 @@ static const unsigned* sort_queue(const TraceParams& p, const WavefrontBuffers& 
     const int grid = grid_cached((const void*)k_wf_sort_keys, tune.block);
     sc.run(kStageSort, p, s, [&](const TraceParams& q) {
         k_wf_sort_keys<<<grid, tune.block, 0, s>>>(q, W, in_q, keys_in);
-        size_t bytes = b.sort_temp_bytes;
-        cub::DeviceRadixSort::SortPairs(b.sort_temp, bytes, keys_in, keys_out, W.q[in_q], sorted, (int)W.slots, 0,
-                                        kSortKeyBits, s);
+        radix_sort_pairs<unsigned>(b.sort_temp, b.sort_temp_bytes, keys_in, keys_out, W.q[in_q], sorted,
+                                   (long long)W.slots, 0, kSortKeyBits, s);
     });
     return sorted;
 }
