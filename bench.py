@@ -383,6 +383,8 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, exact_candidates=True)
     if args.resume_rounds is not None:
         shape = dict(shape, resume_rounds=args.resume_rounds)
+    if args.bvh_builder != "default":
+        shape = dict(shape, bvh_builder=args.bvh_builder)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     backward = S.wl.backward
@@ -800,6 +802,8 @@ def main():
     ap.add_argument("--resume-rounds", type=int, choices=(0, 1, 2), default=None,
                     help="k-buffer rounds resumed from the previous round's frontier: 0 backward replay (default), "
                          "1 none, 2 replay and intersection")
+    ap.add_argument("--bvh-builder", default="default", choices=("default", "morton", "ploc"),
+                    help="hierarchy of the rebuild before the warm-up (the timed steps refit it)")
     ap.add_argument("--exact-candidates", action="store_true",
                     help="every traversal returns exactly the K nearest candidates (order independent)")
     args = ap.parse_args()

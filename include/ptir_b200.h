@@ -31,7 +31,9 @@
  *     outputs are written as zeros).
  *   - The library owns its acceleration structure and scratch; buffers grow, never shrink.
  *   - All work is enqueued on `stream` (a cudaStream_t); no entry point synchronises the host
- *     with the device, so a trace can be captured in a CUDA graph once the structure exists.
+ *     with the device, so a trace can be captured in a CUDA graph once the structure exists. The
+ *     one exception is a rebuild by ptir_build_bvh with the PLOC builder (the default), which
+ *     reads a count back between its iterations; a refit does not.
  *   - Return value: PTIR_OK (0) or a PTIR_E* code; ptir_last_error() describes the last failure.
  *   - A handle is not thread-safe (nor is the reference's object).
  */
@@ -44,7 +46,7 @@
 extern "C" {
 #endif
 
-#define PTIR_ABI_VERSION 5
+#define PTIR_ABI_VERSION 6
 
 enum {
     PTIR_OK = 0,
@@ -119,7 +121,15 @@ typedef struct ptir_config {
                                      from the root (fewer node visits; the same candidates up to the
                                      grazing case above): 0 = the backward replay's (default), 1 =
                                      none, 2 = the replay's and the intersection stage's */
+    int32_t bvh_builder;          /* hierarchy of a rebuild: 0 = default (PTIR_BVH_PLOC), PTIR_BVH_MORTON =
+                                     the Karras hierarchy over the sorted keys, PTIR_BVH_PLOC = agglomerative
+                                     clustering by surface area over the same sorted leaves (a better tree, a
+                                     slower build that synchronises its stream: a rebuild then cannot be
+                                     captured in a CUDA graph, a refit can). The traced results are the same
+                                     up to the order-dependent grazing case of exact_candidates */
 } ptir_config;
+
+enum { PTIR_BVH_DEFAULT = 0, PTIR_BVH_MORTON = 1, PTIR_BVH_PLOC = 2 };
 
 enum { PTIR_STORAGE_FP32 = 0, PTIR_STORAGE_BF16 = 1, PTIR_STORAGE_FP16 = 2 };
 

@@ -11,7 +11,7 @@ from . import build as _build
 
 _LIB = None
 
-ABI_VERSION = 5  # PTIR_ABI_VERSION of include/ptir_b200.h that these structs mirror
+ABI_VERSION = 6  # PTIR_ABI_VERSION of include/ptir_b200.h that these structs mirror
 PTIR_OK = 0
 PTIR_EINVAL = 1
 PTIR_ECUDA = 2
@@ -47,10 +47,12 @@ class PtirConfig(C.Structure):
         ("shadow_kbuffer", C.c_int32),
         ("exact_candidates", C.c_int32),
         ("resume_rounds", C.c_int32),
+        ("bvh_builder", C.c_int32),
     ]
 
 
 STORAGES = {"fp32": 0, "bf16": 1, "fp16": 2}
+BVH_BUILDERS = {"default": 0, "morton": 1, "ploc": 2}
 STAGES = ("intersect", "shadow", "replay", "shading", "megakernel", "sort")
 
 

@@ -7,7 +7,8 @@
 //   3. morton    60-bit extended Morton key: AABB centre and size
 //   4. sort      key/id radix sort (radix_sort.cuh: stable LSD, 8-bit digits)
 //   5. gather    leaf records in key order
-//   6. hierarchy internal nodes from the sorted keys (ties broken by position)
+//   6. hierarchy internal nodes from the sorted keys (ties broken by position), or PLOC
+//                (agglomerative clustering by surface area over the sorted leaves)
 //   7. refit     bottom-up child boxes with arrival counters
 //   8. collapse  4-wide nodes, greedy by surface area (rebuild only)
 //   9. emit      the 4-wide node records the traversal reads
@@ -217,6 +218,188 @@ __global__ void k_hierarchy(int n, const unsigned long long* __restrict__ keys, 
     if (i == 0) parent[0] = -1;
 }
 
+// ---------------------------------------------------------------------------------------
+// PLOC (Meister and Bittner 2018, "Parallel Locally-Ordered Clustering for Bounding Volume
+// Hierarchy Construction"): an agglomerative build over the leaves in key order, in place of
+// k_hierarchy. Every iteration, each cluster finds among the kPlocRadius clusters on either side
+// of it in the current list the one whose union with it has the smallest box surface area;
+// mutual nearest neighbours merge into a new binary node that takes the left one's place, and
+// the list is compacted. Equal areas go to the smaller index, which with the area orders all
+// pairs strictly, so the smallest pair of the list is always mutual and every iteration merges
+// at least one pair. Node indices are handed out from n - 2 down, so the last merge (the root)
+// is node 0 as in the Karras hierarchy, and the binary nodes go through the same refit,
+// collapse and emit.
+constexpr int kPlocRadius = 16;
+constexpr int kPlocThreads = 256;
+constexpr int kPlocScanThreads = 1024;
+constexpr int kPlocBatch = 4;  // iterations launched between reads of the cluster count
+
+// surface area (halved) of the union of two boxes; the same value whichever box comes first
+__device__ __forceinline__ float ploc_area(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+    const float ex = fmaxf(ahi.x, bhi.x) - fminf(alo.x, blo.x);
+    const float ey = fmaxf(ahi.y, bhi.y) - fminf(alo.y, blo.y);
+    const float ez = fmaxf(ahi.z, bhi.z) - fminf(alo.z, blo.z);
+    const float a = ex * ey + ey * ez + ez * ex;
+    return a == a ? a : INFINITY;  // a NaN box still pairs with someone
+}
+
+// the leaves in key order as the first clusters (cid ~i: leaf i), their instance boxes
+__global__ void k_ploc_init(int n, const float4* __restrict__ box, const unsigned* __restrict__ order,
+                            int* __restrict__ cid, float4* __restrict__ cb, unsigned* __restrict__ count,
+                            unsigned* __restrict__ next_node) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        *count = (unsigned)n;
+        *next_node = (unsigned)(n - 1);
+    }
+    if (i >= n) return;
+    const unsigned g = order[i];
+    cid[i] = ~i;
+    cb[2 * (size_t)i] = box[2 * (size_t)g];
+    cb[2 * (size_t)i + 1] = box[2 * (size_t)g + 1];
+}
+
+// nearest neighbour of every cluster within kPlocRadius positions (-1 when alone)
+__global__ void __launch_bounds__(kPlocThreads) k_ploc_nn(const unsigned* __restrict__ count_p,
+                                                          const float4* __restrict__ cb, int* __restrict__ nn) {
+    constexpr int kSpan = kPlocThreads + 2 * kPlocRadius;
+    __shared__ float4 slo[kSpan], shi[kSpan];
+    const int count = (int)*count_p;
+    const int b0 = blockIdx.x * kPlocThreads;
+    if (b0 >= count) return;
+    for (int k = threadIdx.x; k < kSpan; k += kPlocThreads) {
+        const int j = b0 - kPlocRadius + k;
+        if (j >= 0 && j < count) {
+            slo[k] = cb[2 * (size_t)j];
+            shi[k] = cb[2 * (size_t)j + 1];
+        }
+    }
+    __syncthreads();
+    const int i = b0 + threadIdx.x;
+    if (i >= count) return;
+    const int s = threadIdx.x + kPlocRadius;
+    const float4 lo = slo[s], hi = shi[s];
+    int best = -1;
+    float barea = INFINITY;
+    for (int d = -kPlocRadius; d <= kPlocRadius; ++d) {
+        const int j = i + d;
+        if (d == 0 || j < 0 || j >= count) continue;
+        const float a = ploc_area(lo, hi, slo[s + d], shi[s + d]);
+        if (best < 0 || a < barea) {  // j ascends, so an equal area keeps the smaller index
+            barea = a;
+            best = j;
+        }
+    }
+    nn[i] = best;
+}
+
+// number of clusters of a block that stay in the list (all but the right one of each merged pair)
+__device__ __forceinline__ unsigned ploc_block_keep(bool keep, unsigned* wsum) {
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, keep);
+    if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = __popc(bal);
+    __syncthreads();
+    return bal;
+}
+
+// merge of mutual nearest neighbours: a binary node (left, right) with its parent links, in the
+// left cluster's place; per block the number of clusters kept
+__global__ void __launch_bounds__(kPlocThreads) k_ploc_merge(int n, const unsigned* __restrict__ count_p,
+                                                             const int* __restrict__ nn, int* __restrict__ cid,
+                                                             float4* __restrict__ cb, float4* __restrict__ nodes,
+                                                             int* __restrict__ parent, unsigned* __restrict__ next_node,
+                                                             unsigned* __restrict__ blk) {
+    __shared__ unsigned wsum[kPlocThreads / 32];
+    const int count = (int)*count_p;
+    const int b0 = blockIdx.x * kPlocThreads;
+    if (b0 >= count) return;
+    const int i = b0 + threadIdx.x;
+    bool keep = false;
+    if (i < count) {
+        const int j = nn[i];
+        const bool mutual = j >= 0 && nn[j] == i;
+        keep = !(mutual && j < i);
+        if (mutual && i < j) {
+            const int idx = (int)atomicSub(next_node, 1u) - 1;
+            const int l = cid[i], r = cid[j];
+            nodes[4 * (size_t)idx + 3] = make_float4(__int_as_float(l), __int_as_float(r), 0.0f, 0.0f);
+            parent[l < 0 ? (n - 1) + ~l : l] = idx;
+            parent[r < 0 ? (n - 1) + ~r : r] = idx;
+            const float4 alo = cb[2 * (size_t)i], ahi = cb[2 * (size_t)i + 1];
+            const float4 blo = cb[2 * (size_t)j], bhi = cb[2 * (size_t)j + 1];
+            cb[2 * (size_t)i] = make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.0f);
+            cb[2 * (size_t)i + 1] = make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.0f);
+            cid[i] = idx;
+        }
+    }
+    ploc_block_keep(keep, wsum);
+    if (threadIdx.x == 0) {
+        unsigned s = 0;
+        for (int w = 0; w < kPlocThreads / 32; ++w) s += wsum[w];
+        blk[blockIdx.x] = s;
+    }
+}
+
+// exclusive scan of the per-block counts in one block; the total is the next cluster count
+__global__ void __launch_bounds__(kPlocScanThreads) k_ploc_scan(const unsigned* __restrict__ count_p,
+                                                                unsigned* __restrict__ blk,
+                                                                unsigned* __restrict__ count_out) {
+    __shared__ unsigned wsum[kPlocScanThreads / 32];
+    const int count = (int)*count_p;
+    const int nb = (count + kPlocThreads - 1) / kPlocThreads;
+    const unsigned ln = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    unsigned carry = 0;
+    for (int base = 0; base < nb; base += kPlocScanThreads) {
+        const int k = base + (int)threadIdx.x;
+        const unsigned v = k < nb ? blk[k] : 0u;
+        unsigned x = v;  // inclusive scan within the warp
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (ln >= (unsigned)o) x += y;
+        }
+        if (ln == 31) wsum[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            unsigned t = wsum[ln];
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xFFFFFFFFu, t, o);
+                if (ln >= (unsigned)o) t += y;
+            }
+            wsum[ln] = t;
+        }
+        __syncthreads();
+        if (k < nb) blk[k] = carry + (w > 0 ? wsum[w - 1] : 0u) + x - v;
+        carry += wsum[kPlocScanThreads / 32 - 1];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *count_out = carry;
+}
+
+// the kept clusters, in order, into the other list
+__global__ void __launch_bounds__(kPlocThreads) k_ploc_compact(const unsigned* __restrict__ count_p,
+                                                               const int* __restrict__ nn, const int* __restrict__ cid,
+                                                               const float4* __restrict__ cb,
+                                                               const unsigned* __restrict__ blk, int* __restrict__ cid_out,
+                                                               float4* __restrict__ cb_out) {
+    __shared__ unsigned wsum[kPlocThreads / 32];
+    const int count = (int)*count_p;
+    const int b0 = blockIdx.x * kPlocThreads;
+    if (b0 >= count) return;
+    const int i = b0 + threadIdx.x;
+    bool keep = false;
+    if (i < count) {
+        const int j = nn[i];
+        keep = !(j >= 0 && j < i && nn[j] == i);
+    }
+    const unsigned bal = ploc_block_keep(keep, wsum);
+    unsigned off = blk[blockIdx.x] + __popc(bal & ((1u << (threadIdx.x & 31u)) - 1u));
+    for (unsigned w = 0; w < (threadIdx.x >> 5); ++w) off += wsum[w];
+    if (keep) {
+        cid_out[off] = cid[i];
+        cb_out[2 * (size_t)off] = cb[2 * (size_t)i];
+        cb_out[2 * (size_t)off + 1] = cb[2 * (size_t)i + 1];
+    }
+}
+
 // box and kmax of child c of the hierarchy
 __device__ __forceinline__ void child_box(const float4* __restrict__ sbox_unsorted, const unsigned* __restrict__ order,
                                           const float4* nodes, int c, float3& lo, float3& hi, float& kmax) {
@@ -395,6 +578,90 @@ cudaError_t grow(T*& ptr, size_t count, cudaStream_t s) {
     return cudaMallocAsync(reinterpret_cast<void**>(&ptr), count * sizeof(T), s);
 }
 
+// The binary nodes and parent links of a PLOC build over the n > 1 leaves in key order
+// (st.ids[1]). Its scratch lives for the build only. Iterations are launched kPlocBatch at a
+// time, then the cluster count is read back; at most n - 1 iterations are needed, since each
+// merges at least one pair.
+cudaError_t ploc_build(AccelState& st, int n, cudaStream_t s, std::string& err) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cap);
+    if (e != cudaSuccess) {
+        err = std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e);
+        return e;
+    }
+    if (cap != cudaStreamCaptureStatusNone) {
+        err = "a PLOC rebuild reads its cluster count back between iterations and cannot be captured in a CUDA "
+              "graph: rebuild before the capture and refit inside it";
+        return cudaErrorStreamCaptureUnsupported;
+    }
+    if (!st.ploc_host) {
+        e = cudaMallocHost(reinterpret_cast<void**>(&st.ploc_host), 2 * sizeof(unsigned));
+        if (e != cudaSuccess) {
+            err = std::string("cudaMallocHost: ") + cudaGetErrorString(e);
+            return e;
+        }
+    }
+    const int nb = (n + kPlocThreads - 1) / kPlocThreads;
+    // cluster boxes [2][2n] float4, cluster ids [2][n], neighbours [n], block counts [nb], counters [4]
+    const size_t box_bytes = 2 * sizeof(float4) * (size_t)n;
+    const size_t bytes = 2 * box_bytes + (3 * (size_t)n + (size_t)nb + 4) * sizeof(int) + 256;
+    char* scratch = nullptr;
+    e = cudaMallocAsync(reinterpret_cast<void**>(&scratch), bytes, s);
+    if (e != cudaSuccess) {
+        err = std::string("cudaMallocAsync (PLOC scratch): ") + cudaGetErrorString(e);
+        return e;
+    }
+    float4* cb[2] = {reinterpret_cast<float4*>(scratch), reinterpret_cast<float4*>(scratch + box_bytes)};
+    int* cid[2] = {reinterpret_cast<int*>(scratch + 2 * box_bytes), reinterpret_cast<int*>(scratch + 2 * box_bytes) + n};
+    int* nn = cid[1] + n;
+    unsigned* blk = reinterpret_cast<unsigned*>(nn + n);
+    unsigned* cnt = blk + nb;  // [0], [1]: cluster counts of the two lists; [2]: next node index
+    unsigned* next_node = cnt + 2;
+    k_ploc_init<<<nb, kPlocThreads, 0, s>>>(n, st.box, st.ids[1], cid[0], cb[0], cnt, next_node);
+    e = cudaGetLastError();
+    int cur = 0;
+    for (long long it = 0; e == cudaSuccess;) {
+        for (int b = 0; b < kPlocBatch; ++b, ++it) {
+            k_ploc_nn<<<nb, kPlocThreads, 0, s>>>(cnt + cur, cb[cur], nn);
+            k_ploc_merge<<<nb, kPlocThreads, 0, s>>>(n, cnt + cur, nn, cid[cur], cb[cur], st.nodes, st.parent, next_node,
+                                                     blk);
+            k_ploc_scan<<<1, kPlocScanThreads, 0, s>>>(cnt + cur, blk, cnt + 1 - cur);
+            k_ploc_compact<<<nb, kPlocThreads, 0, s>>>(cnt + cur, nn, cid[cur], cb[cur], blk, cid[1 - cur], cb[1 - cur]);
+            cur = 1 - cur;
+        }
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(st.ploc_host, cnt + cur, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(st.ploc_host + 1, next_node, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            err = std::string("PLOC iteration: ") + cudaGetErrorString(e);
+            break;
+        }
+        if (st.ploc_host[0] <= 1u) {
+            if (st.ploc_host[1] != 0u) {  // n - 1 merges hand out every node index
+                err = "PLOC ended with " + std::to_string(st.ploc_host[1]) + " node indices unused";
+                e = cudaErrorUnknown;
+            }
+            break;
+        }
+        if (it > (long long)n + kPlocBatch) {
+            err = "PLOC did not converge";
+            e = cudaErrorUnknown;
+            break;
+        }
+    }
+    if (e == cudaSuccess) {
+        e = cudaMemsetAsync(st.parent, 0xFF, sizeof(int), s);  // the root (node 0) has no parent
+        if (e != cudaSuccess) err = std::string("cudaMemsetAsync: ") + cudaGetErrorString(e);
+    }
+    const cudaError_t f = cudaFreeAsync(scratch, s);
+    if (e == cudaSuccess && f != cudaSuccess) {
+        err = std::string("cudaFreeAsync (PLOC scratch): ") + cudaGetErrorString(f);
+        e = f;
+    }
+    return e;
+}
+
 }  // namespace
 
 cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const float* pos, const float* rot,
@@ -460,7 +727,15 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
         }
         PTIR_TRY(radix_sort_pairs<unsigned long long>(st.sort_temp, st.sort_temp_bytes, st.keys[0], st.keys[1], st.ids[0],
                                                       st.ids[1], n, 0, kKeyBits, s));
-        if (n > 1) {
+        if (n > 1 && opt.builder == kBuilderPloc) {
+            std::string perr;
+            e = ploc_build(st, n, s, perr);
+            if (e != cudaSuccess) {
+                err = perr;
+                st.valid = false;
+                return e;
+            }
+        } else if (n > 1) {
             const unsigned iblocks = (unsigned)((n - 1 + T - 1) / T);
             k_hierarchy<<<iblocks, T, 0, s>>>(n, st.keys[1], st.nodes, st.parent);
             PTIR_TRY(cudaGetLastError());
@@ -508,6 +783,7 @@ void accel_free(AccelState& st) {
     rel(st.wchild);
     rel(st.wcount);
     rel(st.nodes4);
+    if (st.ploc_host) cudaFreeHost(st.ploc_host);
     st = AccelState();
 }
 

@@ -16,7 +16,10 @@ struct AccelBuildOptions {
     float min_response;      // kernel support ends where the (clamped) response reaches this
     int density_clamping;    // adaptive support: the response threshold is divided by the density
     unsigned storage;        // attribute storage (storage.cuh): inputs are rounded to it first
+    unsigned builder;        // kBuilderMorton: Karras hierarchy over the sorted keys; kBuilderPloc: PLOC
 };
+
+enum : unsigned { kBuilderMorton = 0, kBuilderPloc = 1 };
 
 // Device buffers of one acceleration structure; grown on demand, never shrunk.
 struct AccelState {
@@ -39,6 +42,7 @@ struct AccelState {
     float4* nodes4 = nullptr;   // [(n-1)*8] 4-wide nodes traversed by the tracer
     void* sort_temp = nullptr;
     size_t sort_temp_bytes = 0;
+    unsigned* ploc_host = nullptr;  // pinned [2]: cluster count and next node index read back by a PLOC build
     size_t capacity = 0;        // Gaussians the buffers can hold
 
     AccelView view() const { return AccelView{nodes4, leaves, bounds, valid ? n : 0, 0.0f}; }
@@ -46,7 +50,9 @@ struct AccelState {
 
 // Build (rebuild != 0 or topology unusable) or refit the structure from per-Gaussian
 // position [n,3], rotation [n,4] (wxyz), scale [n,3] and density [n,1] (device pointers).
-// Returns a CUDA error code and a message in `err` on failure.
+// Returns a CUDA error code and a message in `err` on failure. A PLOC rebuild reads the cluster
+// count back to the host between its iterations, so it synchronises the stream and cannot be
+// captured in a CUDA graph (a refit can).
 cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const float* pos, const float* rot,
                         const float* scl, const float* dns, int n, bool rebuild, cudaStream_t stream,
                         std::string& err);

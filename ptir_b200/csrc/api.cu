@@ -335,6 +335,9 @@ int ptir_create(const ptir_config* config, ptir_tracer** out) {
     if (config->grad_aggregate != 0 && config->grad_aggregate != 1) return PTIR_EINVAL;
     if (config->exact_candidates != 0 && config->exact_candidates != 1) return PTIR_EINVAL;
     if (config->resume_rounds < 0 || config->resume_rounds > 2) return PTIR_EINVAL;
+    if (config->bvh_builder != PTIR_BVH_DEFAULT && config->bvh_builder != PTIR_BVH_MORTON &&
+        config->bvh_builder != PTIR_BVH_PLOC)
+        return PTIR_EINVAL;
     if (config->storage != PTIR_STORAGE_FP32 && config->storage != PTIR_STORAGE_BF16 &&
         config->storage != PTIR_STORAGE_FP16)
         return PTIR_EINVAL;
@@ -373,7 +376,8 @@ int ptir_build_bvh(ptir_tracer* t, const float* pos, const float* rot, const flo
     if (n < 0) return fail(t, PTIR_EINVAL, "negative particle count");
     if (n > 0 && (!pos || !rot || !scl || !dns)) return fail(t, PTIR_EINVAL, "null particle pointer");
     ptir::AccelBuildOptions opt{t->cfg.kernel_degree, t->cfg.kernel_min_response, t->cfg.density_clamping,
-                                (unsigned)t->cfg.storage};
+                                (unsigned)t->cfg.storage,
+                                t->cfg.bvh_builder == PTIR_BVH_MORTON ? ptir::kBuilderMorton : ptir::kBuilderPloc};
     // the reference refits only when asked and allowed and the count is unchanged (optixTracer.cpp:646-649, 819-822)
     const bool do_rebuild = rebuild != 0 || allow_update == 0 || n != t->accel.n;
     std::string err;

@@ -114,7 +114,10 @@ class OptixTracer:
     the results depend on neither the traversal order nor ``kbuffer``. ``resume_rounds`` (k-buffer 8
     or 16) picks the traversals whose next k-buffer round starts from what the previous round set
     aside against its K-th distance instead of from the root: 0 the backward replay's (default), 1
-    none, 2 the replay's and the intersection stage's."""
+    none, 2 the replay's and the intersection stage's. ``bvh_builder`` picks the hierarchy of a
+    rebuild: "morton" (the Karras hierarchy over the sorted keys), "ploc" (agglomerative clustering
+    by surface area over the same sorted leaves: a better tree and a slower build, which
+    synchronises the stream, so a rebuild cannot be captured in a CUDA graph) or "default" (PLOC)."""
 
     def __init__(
         self,
@@ -147,6 +150,7 @@ class OptixTracer:
         shadow_kbuffer: int = 0,
         exact_candidates: bool = False,
         resume_rounds: int = 0,
+        bvh_builder: str = "default",
     ):
         if pipeline not in ("reference",):
             raise ValueError(f"pipeline '{pipeline}' is not available (only 'reference')")
@@ -164,7 +168,7 @@ class OptixTracer:
             N.SCHEDULES[schedule], int(chunk_tiles), int(kbuffer), int(refill_lanes), int(block_size),
             int(bool(collect_timings)), 0 if sort_rays else 1, int(bool(exact_replay)), 0 if compensated_grads else 1,
             N.STORAGES[storage], 0 if warp_aggregate else 1, int(shadow_kbuffer), int(bool(exact_candidates)),
-            int(resume_rounds))
+            int(resume_rounds), N.BVH_BUILDERS[bvh_builder])
         handle = C.c_void_p()
         rc = self._lib.ptir_create(C.byref(cfg), C.byref(handle))
         if rc != N.PTIR_OK:

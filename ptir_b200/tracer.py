@@ -264,7 +264,7 @@ class Tracer:
         b2 = _conf_get(r, "b200")
         launch = {k: _conf_get(b2, k) for k in ("schedule", "chunk_tiles", "kbuffer", "refill_lanes", "block_size",
                                                  "sort_rays", "storage", "shadow_kbuffer", "exact_candidates",
-                                                 "resume_rounds")}
+                                                 "resume_rounds", "bvh_builder")}
         self.tracer_wrapper = OptixTracer(
             "", "", r.pipeline_type, r.backward_pipeline_type, r.primitive_type, r.particle_kernel_degree,
             r.particle_kernel_min_response, r.particle_kernel_density_clamping, r.particle_radiance_sph_degree,

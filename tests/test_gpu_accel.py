@@ -106,21 +106,23 @@ def _trace(tr, S, build, rebuild):
     dict(n=3000, w=32, h=24, spp=1, max_bounces=3),
     dict(n=4000, w=32, h=24, spp=1, max_bounces=3, layout="cluster_shell", scale_range=(0.002, 0.2)),
 ])
-def test_structure_contains_every_box(cuda_device, case):
+@pytest.mark.parametrize("builder", ["morton", "ploc"])
+def test_structure_contains_every_box(cuda_device, case, builder):
     s = small_scene(**case)
     S = to_torch(s)
-    tr = make_tracer()
+    tr = make_tracer(bvh_builder=builder)
     tr.build_bvh(S["build_pos"], S["build_rot"], S["build_scl"], S["build_dns"], True, True)
     nodes, leaves = (t.numpy() for t in tr.debug_accel())
     _walk(nodes, leaves)
     _oracle_boxes_match(leaves, s)
 
 
-def test_refit_after_motion_matches_rebuild_and_oracle(cuda_device):
+@pytest.mark.parametrize("builder", ["morton", "ploc"])
+def test_refit_after_motion_matches_rebuild_and_oracle(cuda_device, builder):
     s0 = small_scene(n=3000, w=40, h=32, spp=2, max_bounces=3)
     s1 = _moved(s0)
     S0, S1 = to_torch(s0), to_torch(s1)
-    tr = make_tracer()
+    tr = make_tracer(bvh_builder=builder)
     tr.build_bvh(S0["build_pos"], S0["build_rot"], S0["build_scl"], S0["build_dns"], True, True)
     _, topo0 = _walk(*(t.numpy() for t in tr.debug_accel()))
     ids0 = tr.debug_accel()[1].numpy()[:, 12].copy().view(np.uint32)
@@ -131,7 +133,7 @@ def test_refit_after_motion_matches_rebuild_and_oracle(cuda_device):
     assert np.array_equal(topo0, topo1) and np.array_equal(ids0, ids1), "a refit keeps the topology and leaf order"
     _oracle_boxes_match(leaves, s1)
     # a fresh rebuild of the moved scene
-    tr_b = make_tracer()
+    tr_b = make_tracer(bvh_builder=builder)
     out_b, sig_b = _trace(tr_b, S1, build=True, rebuild=True)
     torch.cuda.synchronize()
     assert tr.device_status() == 0 and tr_b.device_status() == 0
@@ -188,6 +190,47 @@ def test_resumed_calls_match_calls_from_the_root(cuda_device, case, kbuffer):
     g = torch.where(torch.from_numpy(same).cuda()[..., None], g, torch.zeros_like(g))
     grads = []
     for tr, out in ((root, out_a), (resumed, out_b)):
+        _, mg, _, _, eg = gpu_trace_bwd(tr, S, list(out), g)
+        grads.append((mg.cpu().numpy(), eg.cpu().numpy()))
+    torch.cuda.synchronize()
+    for a, b in zip(grads[0], grads[1]):
+        rel, cos = K.rel_cos(a, b)
+        assert rel <= 3e-5 and cos >= 0.99999, (rel, cos)
+
+
+@pytest.mark.parametrize("case", [
+    dict(n=3000, w=48, h=40, spp=2, max_bounces=3),
+    dict(n=6000, w=40, h=32, spp=2, max_bounces=4, layout="cluster_shell", scale_range=(0.002, 0.2)),
+    dict(n=40000, w=32, h=24, spp=1, max_bounces=3, layout="cluster_shell", scale_range=(0.002, 0.2)),
+])
+def test_ploc_tree_traces_as_the_morton_tree(cuda_device, case):
+    """The PLOC hierarchy (agglomerative clustering by surface area, accel.cu) against the Karras
+    hierarchy over the same sorted leaves: every trace call returns the K nearest candidates of its
+    interval whatever the tree, so the paths take the same decisions and their outputs are bitwise
+    equal, up to the order-dependent grazing case. The forward and the adjoint are compared."""
+    s = small_scene(**case)
+    S = to_torch(s)
+    morton = make_tracer(bvh_builder="morton", collect_counters=True)
+    ploc = make_tracer(bvh_builder="ploc", collect_counters=True)
+    out_a, sig_a = _trace(morton, S, build=True, rebuild=True)
+    out_b, sig_b = _trace(ploc, S, build=True, rebuild=True)
+    torch.cuda.synchronize()
+    assert morton.device_status() == 0 and ploc.device_status() == 0
+    _walk(*(t.numpy() for t in ploc.debug_accel()))
+    same = sig_a == sig_b
+    ca, cb = morton.counters(), ploc.counters()
+    print(f"{case}: {same.mean():.6f} of paths take the same decisions; node visits / leaf tests "
+          f"morton {ca['node_visits']} / {ca['leaf_tests']}, ploc {cb['node_visits']} / {cb['leaf_tests']}")
+    assert same.mean() >= 0.999, same.mean()
+    for k in (0, 1, 2, 3, 4, 5, 6, 7, 8, 10, 11, 12):
+        a = out_a[k].cpu().numpy().reshape(*sig_a.shape, -1)
+        b = out_b[k].cpu().numpy().reshape(*sig_b.shape, -1)
+        eq = np.all(a == b, axis=-1)
+        assert eq[same].mean() >= 0.999, (k, eq[same].mean())
+    g = torch.from_numpy(np.random.default_rng(5).standard_normal(tuple(sig_a.shape) + (3,)).astype(np.float32)).cuda()
+    g = torch.where(torch.from_numpy(same).cuda()[..., None], g, torch.zeros_like(g))
+    grads = []
+    for tr, out in ((morton, out_a), (ploc, out_b)):
         _, mg, _, _, eg = gpu_trace_bwd(tr, S, list(out), g)
         grads.append((mg.cpu().numpy(), eg.cpu().numpy()))
     torch.cuda.synchronize()

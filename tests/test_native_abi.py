@@ -26,7 +26,7 @@ def test_library_exports_header_symbols():
 
 def test_abi_version_without_gpu():
     lib = _native.load()
-    assert lib.ptir_abi_version() == _native.ABI_VERSION == 5
+    assert lib.ptir_abi_version() == _native.ABI_VERSION == 6
 
 
 def test_built_for_sm100a():
