@@ -331,7 +331,7 @@ PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, fl
 // tested in between (in the lane, or by the whole warp).
 struct NodeVisit {
     int ch[4];           // children: >= 0 node, kNoChild empty, else leaf ~c
-    float t0[4], key[4]; // cull distance (clipped entry, less the slack), middle of the clipped interval (x2)
+    float t0[4], key[4]; // cull distance (clipped entry, less the slack), visit order key
     unsigned hits;       // children whose box the ray crosses and whose cull distance is before t_K
 };
 
@@ -379,9 +379,11 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const 
         const float b = min3f(fmaf(fxa[k], inv.x, -oi.x), fmaf(fya[k], inv.y, -oi.y),
                               fminf(fmaf(fza[k], inv.z, -oi.z), tend));
         v.t0[k] = kSlack ? a - sl[k] : a;
-        // nearer middle of the clipped interval first: boxes that contain the origin all
-        // enter at tmin, their extent along the ray tells them apart
-        v.key[k] = a + b;
+        // visit order: the clipped entry, with a sixteenth of the clipped extent added so that
+        // boxes that all enter at tmin (those containing the origin) go shorter first. Measured
+        // on 2 views of 512x384x4 (1M Gaussians): the step took 163.7 ms with this key, 171.0
+        // with the entry alone, 168.0 with a quarter of the extent and 178.6 with the middle.
+        v.key[k] = 15.0f * a + b;
         const bool crossed = v.ch[k] != kNoChild && a <= b;
         const bool h = crossed && v.t0[k] <= kt[K - 1];
         if constexpr (kResume) {
@@ -393,8 +395,8 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const 
     return leaves;
 }
 
-// Descent after the leaf tests: into the nearest internal child still in front of the K-th
-// distance, the others pushed farthest first; else the next stacked subtree that can still hold
+// Descent after the leaf tests: into the first internal child by key still in front of the K-th
+// distance, the others pushed largest key first; else the next stacked subtree that can still hold
 // a nearer candidate (then, with kResume, the next frontier entry that can). Returns false when
 // no node visit remains. With kResume what is passed over for the K-th distance is set aside.
 template <int K, bool kResume = false>
@@ -426,7 +428,7 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
             return false;
         }
         while (inner) {
-            // farthest remaining first
+            // largest remaining key first
             int far = -1;
             float fkey = -3.0e38f;
 #pragma unroll
