@@ -28,6 +28,16 @@
 // rejected under a later tmin. The next call processes the frontier's entries in order, those
 // still past its own K-th distance going to its own frontier. The candidates are those of a call
 // from the root (up to the order-dependent grazing case above), with about half the node visits.
+//
+// Seeded calls (TraceState::cap): a caller that can estimate where the call's K-th candidate lies
+// (the wavefront kernel does for a segment's later rounds, from the previous round's span) starts
+// the call with that distance as its cut, so that subtrees past it are culled before the k-buffer
+// is full. A call that fills its k-buffer below the seed has its K nearest candidates. One that
+// does not (fewer than K candidates before the seed) holds every candidate before the seed and is
+// continued past it (TraceState::floor = the seed, no cap): subtrees whose clipped box ends before
+// the floor are culled and leaves need t* >= floor. Both passes keep the reference's candidate
+// test; only the grazing case above (a closest approach outside the Gaussian's own box interval)
+// can be culled by one order and kept by another.
 #pragma once
 
 #include "device_types.h"
@@ -134,7 +144,7 @@ PTIR_DEV bool instance_hit(float3 od, float3 dd, float tmin, float tmax, float& 
 // invokes its intersection program only for instances whose unit box the ray crosses within the
 // current interval, so the box test is part of the candidate test.
 PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float cut,
-                             float& ts_out, unsigned& id_out) {
+                             float& ts_out, unsigned& id_out, float floor = -kFarT) {
     const float4* rec = A.leaves + 4 * (size_t)p;
     const float4 r0 = __ldg(rec + 0), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
     const float3 od = make_float3(r0.x * o.x + r0.y * o.y + r0.z * o.z + r0.w,
@@ -147,7 +157,7 @@ PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, floa
     // the perpendicular distance of instance_hit (almost never the deciding one)
     const float den = 1.0f / dot(dd, dd);
     const float ts = -dot(od, dd) * den;
-    if (!(ts > tmin && ts < fminf(tend, cut))) return false;
+    if (!(ts > tmin && ts >= floor && ts < fminf(tend, cut))) return false;
     const float3 inv = make_float3(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
     float b0, b1;
     slab(f3(-1.0f), f3(1.0f), od, inv, b0, b1);
@@ -160,13 +170,15 @@ PTIR_DEV bool leaf_candidate(const AccelView& A, int p, float3 o, float3 d, floa
 }
 
 // exact instance test of leaf record p, inserted into the k-buffer when it is a candidate: as its
-// Gaussian id, or with kLeafIndex as the leaf record's index (leaf_gaussian maps it to the id)
+// Gaussian id, or with kLeafIndex as the leaf record's index (leaf_gaussian maps it to the id).
+// A seeded call passes its cap, a continued one its floor.
 template <int K, bool kLeafIndex = false, class Ids>
 PTIR_DEV void test_leaf(const AccelView& A, int p, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
-                        Ids& kid) {
+                        Ids& kid, float cap = kFarT, float floor = -kFarT) {
     float ts;
     unsigned gid;
-    if (leaf_candidate(A, p, o, d, tmin, tend, kt[K - 1], ts, gid)) kbuf_insert(kt, kid, ts, kLeafIndex ? (unsigned)p : gid);
+    if (leaf_candidate(A, p, o, d, tmin, tend, fminf(kt[K - 1], cap), ts, gid, floor))
+        kbuf_insert(kt, kid, ts, kLeafIndex ? (unsigned)p : gid);
 }
 
 // Gaussian id of leaf record p
@@ -195,6 +207,8 @@ struct TraceState {
     float3 inv;
     float tmin, tend;
     float slack;  // cull_slack / |d|: a child's cull distance is its box entry less slack * its kmax
+    float cap;    // seeded calls: the cut until the k-buffer is full (kFarT: none)
+    float floor;  // continued calls: candidates have t* >= floor, subtrees ending before it are culled
     int node, sp;
     // resumed calls: which of the lane's two frontier buffers is read, its entries, the next one to
     // read, and the entries set aside so far for the next call (more than the capacity: overflowed)
@@ -281,10 +295,14 @@ PTIR_DEV void test_leaf_resume(const AccelView& A, int p, float3 o, float3 d, Tr
 // Start a trace call of ray (o, d) over (tmin, tend). Returns true when node visits remain
 // (trace_step), false when (kt, kid) is already final. With kResume (k-buffer of leaf record
 // indices, frontier F) a call with `resume` continues from what the segment's previous call set
-// aside, unless that overflowed F; a segment's first call starts from the root.
+// aside, unless that overflowed F; a segment's first call starts from the root. `cap` seeds the
+// call's cut (trace_continue takes over a seeded call that ends with its k-buffer not full).
 template <int K, bool kLeafIndex = false, bool kResume = false, class Ids>
 PTIR_DEV bool trace_start(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K], Ids& kid,
-                          TraceState& t, TraceCounters& ctr, const Frontier* F = nullptr, bool resume = false) {
+                          TraceState& t, TraceCounters& ctr, const Frontier* F = nullptr, bool resume = false,
+                          float cap = kFarT) {
+    t.cap = cap;
+    t.floor = -kFarT;
     static_assert(!kResume || kLeafIndex, "resumed calls keep leaf record indices in the k-buffer");
     if constexpr (kResume) {
         if (!resume) {
@@ -384,8 +402,10 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const 
         // on 2 views of 512x384x4 (1M Gaussians): the step took 163.7 ms with this key, 171.0
         // with the entry alone, 168.0 with a quarter of the extent and 178.6 with the middle.
         v.key[k] = 15.0f * a + b;
-        const bool crossed = v.ch[k] != kNoChild && a <= b;
-        const bool h = crossed && v.t0[k] <= kt[K - 1];
+        // a continued call also culls what ends before its floor (t* lies in the box interval,
+        // up to the grazing case; with the slack, within the slack of it)
+        const bool crossed = v.ch[k] != kNoChild && a <= b && (kSlack ? b + sl[k] : b) >= t.floor;
+        const bool h = crossed && v.t0[k] <= fminf(kt[K - 1], t.cap);
         if constexpr (kResume) {
             if (crossed && !h) defer(*F, t, v.ch[k], v.t0[k]);
         }
@@ -410,7 +430,7 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         const bool cand = ((v.hits >> k) & 1u) && v.ch[k] >= 0;
-        const bool h = cand && v.t0[k] <= kt[K - 1];
+        const bool h = cand && v.t0[k] <= fminf(kt[K - 1], t.cap);
         if constexpr (kResume) {
             if (cand && !h) defer(*F, t, v.ch[k], v.t0[k]);  // passed over after the leaf tests
         }
@@ -449,7 +469,7 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
         bool found = false;
         while (sp > 0) {
             --sp;
-            if (stack_t[sp] <= kt[K - 1]) {
+            if (stack_t[sp] <= fminf(kt[K - 1], t.cap)) {
                 node = stack[sp];
                 found = true;
                 break;
@@ -490,11 +510,23 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
         const int c = k == 0 ? v.ch[0] : (k == 1 ? v.ch[1] : (k == 2 ? v.ch[2] : v.ch[3]));
         ++ctr.leaves;
         if constexpr (kResume) test_leaf_resume(A, ~c, o, d, t, kt, kid, *F);
-        else test_leaf<K, kLeafIndex>(A, ~c, o, d, t.tmin, t.tend, kt, kid);
+        else test_leaf<K, kLeafIndex>(A, ~c, o, d, t.tmin, t.tend, kt, kid, t.cap, t.floor);
     }
     if (descend<K, kResume>(t, v, kt, stack, stack_t, err, ctr, F)) return true;
     ctr.candidates += kbuf_count(kt);
     return false;
+}
+
+// A seeded call that ended with its k-buffer not full holds every candidate before its cap: it
+// goes on from the root for the candidates from the cap on, keeping its k-buffer (the same call:
+// its candidates are counted when it ends again).
+template <int K>
+PTIR_DEV void trace_continue(TraceState& t, const float (&kt)[K], TraceCounters& ctr) {
+    ctr.candidates -= kbuf_count(kt);
+    t.floor = t.cap;
+    t.cap = kFarT;
+    t.node = 0;
+    t.sp = 0;
 }
 
 // Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
