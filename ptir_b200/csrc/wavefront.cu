@@ -220,10 +220,12 @@ struct Parked {
 // than 168 (three blocks); 96 (five blocks) was 23 % slower.
 constexpr int trace_regs(int K) { return K > 16 ? 128 : 96; }
 
-// Seed of a segment's later k-buffer rounds in the intersection stage: the cut starts at the round's
-// tmin plus this multiple of the previous round's span (its K-th less its first distance). On 2 views
-// of 512x384x4 (1M Gaussians) 17 % of the seeded rounds were continued past the seed at 2, and the
-// step took 150.9 ms, against 163.8 ms unseeded, 154.6 ms at 1.5 and 154.1 ms at 3.
+// Seed of the k-buffer rounds in the intersection stage: the cut starts at the round's tmin plus
+// this multiple of a span, the previous round's (its K-th less its first distance) for a segment's
+// later rounds. On 2 views of 512x384x4 (1M Gaussians) 17 % of those rounds were continued past
+// the seed at 2, and the step took 150.9 ms, against 163.8 ms unseeded, 154.6 ms at 1.5 and 154.1
+// ms at 3. Seeding the first rounds as well (from the lane's last segment) took it to 142.0 ms (5.6 %
+// of them continued), against 145.5 ms at 1.5 and 143.2 ms at 3.
 constexpr float kSeedSpan = 2.0f;
 
 //
@@ -266,14 +268,17 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
     float3 ro = f3(0.0f), rd = f3(0.0f);  // the lane's segment ray
     TraceState t;
     bool seeded = false;  // the lane's call started with a cut estimated from its previous round
+    float first_span = 0.0f;  // K-th distance less tmin of the first round of the lane's last segment
     float kt[K];  // a call found nothing when kt[0] == kFarT
     unsigned kid[K];
-    // next trace call of this lane's segment, or ready with nothing found when it is complete. A
-    // round after the segment's first (the reference's k-buffer of 16, from the root) is seeded with
-    // the cut tmin + kSeedSpan x the previous round's span of distances (traverse.cuh: a call that
-    // does not fill its k-buffer below it is continued past it). Rounds of 8 are not seeded: their
-    // spans are short, and a seed that close culls more grazing Gaussians (0.17 % of the paths
-    // changed on a scene of Gaussians up to 0.3 in size).
+    // next trace call of this lane's segment, or ready with nothing found when it is complete. The
+    // rounds of the reference's k-buffer of 16 (from the root) are seeded (traverse.cuh: a call that
+    // does not fill its k-buffer below its seed is continued past it): a segment's later round with
+    // the cut tmin + kSeedSpan x the previous round's span of distances, its first round with tmin +
+    // kSeedSpan x the first-round span (K-th distance less tmin) of the lane's last segment, a
+    // neighbouring ray in the queue's order. Rounds of 8 are not seeded: their spans are short, and
+    // a seed that close culls more grazing Gaussians (0.17 % of the paths changed on a scene of
+    // Gaussians up to 0.3 in size).
     auto next_call = [&](const Composite& c) {
         if (!composite_open(P, c)) {
             kt[0] = kFarT;
@@ -289,9 +294,10 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
         float cap = kFarT;
         seeded = false;
         if constexpr (!kIdx && K == 16) {
-            if (rounds > 1) {
-                // kt still holds the previous round, a full k-buffer
-                cap = composite_tmin(c) + kSeedSpan * (kt[K - 1] - kt[0]);
+            // kt still holds the previous round (a full k-buffer) when there is one
+            const float span = rounds > 1 ? kt[K - 1] - kt[0] : first_span;
+            if (span > 0.0f) {
+                cap = composite_tmin(c) + kSeedSpan * span;
                 seeded = cap < composite_tend(c);
                 if (!seeded) cap = kFarT;
             }
@@ -389,6 +395,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
                     else
                         composite_hits_strided<kSelfOcc, K>(P, ctr, c, batch_t, batch_id, nthreads, mark);
                     // a k-buffer that is not full held every candidate of the call: a later call finds none
+                    if (rounds == 1 && kid[K - 1] != kNoHit) first_span = kt[K - 1] - t.tmin;
                     if (kid[K - 1] != kNoHit) next_call(c);
                     else no_call();
                 }
