@@ -318,8 +318,8 @@ def _view_config(views):
 # camera (the 1M-Gaussian scene's opaque shell keeps its pbr image black).
 LOSS_L1, LOSS_ALBEDO, LOSS_ROUGHNESS = 0.8, 0.5, 0.2
 # dram__bytes_read.sum + dram__bytes_write.sum of k_wf_trace per segment it intersects, from an ncu
-# capture of 16 launches on 2 views of 512x384x4 (1,232,548,608 bytes over ~1,652,977 segments)
-DRAM_BYTES_PER_INTERSECT_SEGMENT = 745.7
+# capture of 16 launches on 2 views of 512x384x4 (1,184,413,952 bytes over ~1,652,977 segments)
+DRAM_BYTES_PER_INTERSECT_SEGMENT = 716.5
 STEP_DESC = ("lbvh refit + forward + loss (0.8 L1(pbr, target) + 0.5 L2(albedo, prior) + 0.2 L2(roughness, prior)) "
              "+ adjoint + selective adam (material, env)")
 
