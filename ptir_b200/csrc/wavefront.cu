@@ -519,16 +519,32 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, 
     float start = 0.0f, end = 0.0f;
     Pcg32 rng;
     TraceState t;
+    bool seeded = false;      // the lane's call started with a cut estimated from a span, as in k_wf_trace
+    float first_span = 0.0f;  // K-th distance less tmin of the first round of the lane's last shadow ray
     float kt[K];
     unsigned kid[K];
-    // next trace call of the lane's ray over (start, end), or the ray is decided (unoccluded)
+    // next trace call of the lane's ray over (start, end), or the ray is decided (unoccluded). Rounds
+    // of 16 are seeded as in k_wf_trace: a later round from the previous round's span, a first round
+    // from the first-round span of the lane's last shadow ray (a neighbour in the sorted queue).
     auto next_call = [&]() -> bool {
         if (!(start < end)) return false;
         if (++rounds > (1 << 16) + 1) {
             atomicOr(P.error_word, kErrLoopBound);
             return false;
         }
-        phase = trace_start(P.accel, ro, rd, start + 1e-9f, end, kt, kid, t, ctr) ? kTracing : kReady;
+        float cap = kFarT;
+        seeded = false;
+        if constexpr (K == 16) {
+            // kt still holds the previous round (a full k-buffer) when there is one
+            const float span = rounds > 1 ? kt[K - 1] - kt[0] : first_span;
+            if (span > 0.0f) {
+                cap = start + 1e-9f + kSeedSpan * span;
+                seeded = cap < end;
+                if (!seeded) cap = kFarT;
+            }
+        }
+        phase = trace_start(P.accel, ro, rd, start + 1e-9f, end, kt, kid, t, ctr, nullptr, false, cap) ? kTracing
+                                                                                                       : kReady;
         return true;
     };
     while (true) {
@@ -569,11 +585,18 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, 
             const unsigned tracing = __ballot_sync(kFull, phase == kTracing && !done);
             if (!tracing || __popc(eligible & ~tracing) >= refill) break;
             if (phase == kTracing && !done &&
-                !trace_step(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr))
-                phase = kReady;
+                !trace_step(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr)) {
+                if (seeded && kid[K - 1] == kNoHit) {
+                    seeded = false;
+                    trace_continue(t, kt, ctr);
+                } else {
+                    phase = kReady;
+                }
+            }
         }
         // walk the finished batches: the first hit that occludes decides the ray
         if (phase == kReady && !done) {
+            if (rounds == 1 && kid[K - 1] != kNoHit) first_span = kt[K - 1] - t.tmin;
             if (kid[0] == kNoHit) {
                 done = true;
             } else {
