@@ -101,10 +101,9 @@ __global__ void k_env_bwd(int n, const float* in, float* out, TraceParams P, flo
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float* a = in + 6 * i;
-    int stack[1];
-    float stack_t[1];
+    StackEntry stack[1];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    CtxT<16> C{P, stack, stack_t, ctr};
+    CtxT<16> C{P, stack, ctr};
     BwdInputs B{};
     B.environment_grad = env_grad;
     float3 dir_grad = f3(0.0f);

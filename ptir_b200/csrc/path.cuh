@@ -66,8 +66,7 @@ template <int K_>
 struct CtxT {
     static constexpr int K = K_;  // k-buffer size of the traversals
     const TraceParams& P;
-    int* stack;
-    float* stack_t;
+    StackEntry* stack;
     TraceCounters& ctr;
 };
 
@@ -190,7 +189,7 @@ PTIR_DEV bool shadow_occluded(const Ctx& C, float3 o, float3 d, float tmax, Pcg3
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
-        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
+        trace_kbuf(P.accel, o, d, start + 1e-9f, end, kt, kid, C.stack, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
         float batch_end = start;
         bool stop = false;
@@ -634,7 +633,7 @@ PTIR_DEV void intersect_mark(const Ctx& C, Segment& s, Pcg32& rng, float* vis) {
             atomicOr(P.error_word, kErrLoopBound);
             break;
         }
-        trace_kbuf(P.accel, c.o, c.d, composite_tmin(c), composite_tend(c), kt, kid, C.stack, C.stack_t, P.error_word,
+        trace_kbuf(P.accel, c.o, c.d, composite_tmin(c), composite_tend(c), kt, kid, C.stack, P.error_word,
                    C.ctr);
         if (kid[0] == kNoHit) break;
         composite_hits<kSelfOcc>(P, C.ctr, c, kt, kid, vis);
@@ -792,7 +791,7 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const Repla
             if (F) {
                 if (trace_start<K, true, true>(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, t, C.ctr, F,
                                                round > 0)) {
-                    while (trace_step<K, true, true>(P.accel, r.o, r.d, t, kt, kid, C.stack, C.stack_t, P.error_word,
+                    while (trace_step<K, true, true>(P.accel, r.o, r.d, t, kt, kid, C.stack, P.error_word,
                                                      C.ctr, F)) {
                     }
                 }
@@ -802,7 +801,7 @@ PTIR_DEV void replay_material_grad(const Ctx& C, const BwdInputs& B, const Repla
                 continue;
             }
         }
-        trace_kbuf(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, C.stack, C.stack_t, P.error_word, C.ctr);
+        trace_kbuf(P.accel, r.o, r.d, r.start + 1e-9f, r.end, kt, kid, C.stack, P.error_word, C.ctr);
         if (kid[0] == kNoHit) break;
         replay_batch(P, B, r, kt, kid, C.ctr);
         if (kid[K - 1] == kNoHit) break;

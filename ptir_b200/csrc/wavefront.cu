@@ -105,10 +105,9 @@ PTIR_DEV void write_pbr(const FwdOutputs& O, size_t li, const PathState& ps) {
 }
 
 #define PTIR_STAGE_PROLOGUE                         \
-    int stack[kStackDepth];                         \
-    float stack_t[kStackDepth];                     \
+    StackEntry stack[kStackDepth];                     \
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0}; \
-    CtxT<K> C{P, stack, stack_t, ctr};
+    CtxT<K> C{P, stack, ctr};
 
 // ---------------------------------------------------------------------------------------
 // ray order
@@ -255,8 +254,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
     const Parked pk{base, nthreads};
     float* const batch_t = base + kParkedFields * nthreads;
     unsigned* const batch_id = reinterpret_cast<unsigned*>(batch_t + K * nthreads);
-    int stack[kStackDepth];
-    float stack_t[kStackDepth];
+    StackEntry stack[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     constexpr unsigned kFull = 0xFFFFFFFFu;
     enum : int { kIdle = 0, kTracing = 1, kReady = 2 };
@@ -347,7 +345,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_trace(TraceParams P, float* vis,
             const unsigned tracing = __ballot_sync(kFull, phase == kTracing);
             if (!tracing || __popc(eligible & ~tracing) >= refill) break;
             if (phase == kTracing &&
-                !trace_step<K, kIdx, kResume, kSlack>(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr,
+                !trace_step<K, kIdx, kResume, kSlack>(P.accel, ro, rd, t, kt, kid, stack, P.error_word, ctr,
                                                       &F)) {
                 if (seeded && kid[K - 1] == kNoHit) {
                     seeded = false;
@@ -505,8 +503,7 @@ __global__ void __launch_bounds__(kMaxThreads) k_wf_fwd_primary(TraceParams P, F
 // intersection kernel (more resident warps) by 6 % more.
 template <int K>
 __global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, int refill, const unsigned* items) {
-    int stack[kStackDepth];
-    float stack_t[kStackDepth];
+    StackEntry stack[kStackDepth];
     TraceCounters ctr = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     constexpr unsigned kFull = 0xFFFFFFFFu;
     enum : int { kIdle = 0, kTracing = 1, kReady = 2 };
@@ -585,7 +582,7 @@ __global__ void __maxnreg__(trace_regs(K)) k_wf_shadow(TraceParams P, WfView W, 
             const unsigned tracing = __ballot_sync(kFull, phase == kTracing && !done);
             if (!tracing || __popc(eligible & ~tracing) >= refill) break;
             if (phase == kTracing && !done &&
-                !trace_step(P.accel, ro, rd, t, kt, kid, stack, stack_t, P.error_word, ctr)) {
+                !trace_step(P.accel, ro, rd, t, kt, kid, stack, P.error_word, ctr)) {
                 if (seeded && kid[K - 1] == kNoHit) {
                     seeded = false;
                     trace_continue(t, kt, ctr);
