@@ -583,17 +583,7 @@ cudaError_t grow(T*& ptr, size_t count, cudaStream_t s) {
 // time, then the cluster count is read back; at most n - 1 iterations are needed, since each
 // merges at least one pair.
 cudaError_t ploc_build(AccelState& st, int n, cudaStream_t s, std::string& err) {
-    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-    cudaError_t e = cudaStreamIsCapturing(s, &cap);
-    if (e != cudaSuccess) {
-        err = std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e);
-        return e;
-    }
-    if (cap != cudaStreamCaptureStatusNone) {
-        err = "a PLOC rebuild reads its cluster count back between iterations and cannot be captured in a CUDA "
-              "graph: rebuild before the capture and refit inside it";
-        return cudaErrorStreamCaptureUnsupported;
-    }
+    cudaError_t e = cudaSuccess;
     if (!st.ploc_host) {
         e = cudaMallocHost(reinterpret_cast<void**>(&st.ploc_host), 2 * sizeof(unsigned));
         if (e != cudaSuccess) {
@@ -681,6 +671,16 @@ cudaError_t accel_build(AccelState& st, const AccelBuildOptions& opt, const floa
         return cudaErrorInvalidValue;
     }
     const bool refit = !rebuild && st.valid && st.n == n && n > 1;
+    if (!refit && n > 1 && opt.builder == kBuilderPloc) {
+        // refuse before anything is enqueued: a PLOC rebuild synchronises its stream
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        PTIR_TRY(cudaStreamIsCapturing(s, &cap));
+        if (cap != cudaStreamCaptureStatusNone) {
+            err = "a PLOC rebuild reads its cluster count back between iterations and cannot be captured in a CUDA "
+                  "graph: rebuild before the capture and refit inside it";
+            return cudaErrorStreamCaptureUnsupported;
+        }
+    }
     if (!st.bounds) PTIR_TRY(cudaMallocAsync(reinterpret_cast<void**>(&st.bounds), 2 * sizeof(float4), s));
     if (!st.partial) PTIR_TRY(cudaMallocAsync(reinterpret_cast<void**>(&st.partial), 2 * kReduceBlocks * sizeof(float4), s));
     st.n = n;

@@ -237,3 +237,27 @@ def test_ploc_tree_traces_as_the_morton_tree(cuda_device, case):
     for a, b in zip(grads[0], grads[1]):
         rel, cos = K.rel_cos(a, b)
         assert rel <= 1e-5 and cos >= 0.99999, (rel, cos)
+
+
+def test_ploc_rebuild_under_capture_fails_cleanly(cuda_device):
+    """A PLOC rebuild synchronises its stream, so under CUDA-graph capture ptir_build_bvh refuses it
+    before it enqueues anything: the call raises, the capture ends empty, and the structure built
+    before stays in use (the same traces as before the attempt)."""
+    from ptir_b200._native import PtirError
+
+    s = small_scene(n=2000, w=16, h=16, spp=1, max_bounces=2)
+    S = to_torch(s)
+    tr = make_tracer(bvh_builder="ploc")
+    out0, sig0 = _trace(tr, S, build=True, rebuild=True)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with pytest.raises(PtirError, match="cannot be captured"):
+        with torch.cuda.graph(graph):
+            tr.build_bvh(S["build_pos"], S["build_rot"], S["build_scl"], S["build_dns"], True, True)
+    torch.cuda.synchronize()
+    del graph
+    out1, sig1 = _trace(tr, S, build=False, rebuild=False)
+    torch.cuda.synchronize()
+    assert tr.device_status() == 0
+    assert np.array_equal(sig0, sig1)
+    assert torch.equal(out0[10], out1[10])
