@@ -385,6 +385,10 @@ def run_ours(args, rank, world, device):
         shape = dict(shape, resume_rounds=args.resume_rounds)
     if args.bvh_builder != "default":
         shape = dict(shape, bvh_builder=args.bvh_builder)
+    if args.refill_lanes:
+        shape = dict(shape, refill_lanes=args.refill_lanes)
+    if args.block_size:
+        shape = dict(shape, block_size=args.block_size)
     tr = S.tracer(collect_timings=True, storage=args.storage, **shape)
     stream = torch.cuda.current_stream()
     backward = S.wl.backward
@@ -802,6 +806,9 @@ def main():
     ap.add_argument("--resume-rounds", type=int, choices=(0, 1, 2), default=None,
                     help="k-buffer rounds resumed from the previous round's frontier: 0 backward replay (default), "
                          "1 none, 2 replay and intersection")
+    ap.add_argument("--refill-lanes", type=int, default=0, help="waiting lanes before a warp refills (0: tuned / 32)")
+    ap.add_argument("--block-size", type=int, default=0, choices=(0, 64, 128, 256),
+                    help="threads per block of the wavefront stages (0: tuned / 128)")
     ap.add_argument("--bvh-builder", default="default", choices=("default", "morton", "ploc"),
                     help="hierarchy of the rebuild before the warm-up (the timed steps refit it)")
     ap.add_argument("--exact-candidates", action="store_true",
