@@ -1,5 +1,6 @@
-// LBVH build and refit (Karras 2012, "Maximizing Parallelism in the Construction of BVHs,
-// Octrees, and k-d Trees"), specialised to the Gaussian instance boxes of the tracer.
+// BVH build and refit over the Gaussian instance boxes of the tracer: Morton-sorted leaves, then
+// PLOC (Meister and Bittner 2018, the default) or the Karras hierarchy (Karras 2012, "Maximizing
+// Parallelism in the Construction of BVHs, Octrees, and k-d Trees"), collapsed to 4-wide nodes.
 //
 //   1. prep      per Gaussian: kernel support scale, world->instance map, instance AABB
 //                (the instance transform of threedgptir_tracer/src/particlePrimitives.cu:543-610)
