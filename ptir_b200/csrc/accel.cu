@@ -225,9 +225,10 @@ __global__ void k_hierarchy(int n, const unsigned long long* __restrict__ keys, 
 // k_hierarchy. Every iteration, each cluster finds among the kPlocRadius clusters on either side
 // of it in the current list the one whose union with it has the smallest box surface area;
 // mutual nearest neighbours merge into a new binary node that takes the left one's place, and
-// the list is compacted. Equal areas go to the smaller index, which with the area orders all
-// pairs strictly, so the smallest pair of the list is always mutual and every iteration merges
-// at least one pair. Node indices are handed out from n - 2 down, so the last merge (the root)
+// the list is compacted. Equal areas go to the nearer position in the list, then to the pair
+// whose lower index is even, then to the smaller index: with the area this orders all pairs
+// strictly, so the smallest pair of the list is always mutual and every iteration merges at
+// least one pair, and coincident Gaussians (equal boxes) pair up all at once. Node indices are handed out from n - 2 down, so the last merge (the root)
 // is node 0 as in the Karras hierarchy, and the binary nodes go through the same refit,
 // collapse and emit.
 constexpr int kPlocRadius = 16;
@@ -280,15 +281,24 @@ __global__ void __launch_bounds__(kPlocThreads) k_ploc_nn(const unsigned* __rest
     if (i >= count) return;
     const int s = threadIdx.x + kPlocRadius;
     const float4 lo = slo[s], hi = shi[s];
-    int best = -1;
+    int best = -1, bdist = 0, bmin = 0;
     float barea = INFINITY;
     for (int d = -kPlocRadius; d <= kPlocRadius; ++d) {
         const int j = i + d;
         if (d == 0 || j < 0 || j >= count) continue;
         const float a = ploc_area(lo, hi, slo[s + d], shi[s + d]);
-        if (best < 0 || a < barea) {  // j ascends, so an equal area keeps the smaller index
+        const int dist = d < 0 ? -d : d, mn = min(i, j);
+        // pairs ordered by (area, list distance, parity of the lower index, lower index): equal
+        // boxes (coincident Gaussians) then pair up as (0,1), (2,3), ... and halve every
+        // iteration, where the smaller index alone would merge one pair an iteration
+        const bool better = best < 0 || a < barea ||
+                            (a == barea && (dist < bdist || (dist == bdist && ((mn & 1) < (bmin & 1) ||
+                                                                               ((mn & 1) == (bmin & 1) && mn < bmin)))));
+        if (better) {
             barea = a;
             best = j;
+            bdist = dist;
+            bmin = mn;
         }
     }
     nn[i] = best;

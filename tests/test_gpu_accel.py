@@ -261,3 +261,37 @@ def test_ploc_rebuild_under_capture_fails_cleanly(cuda_device):
     assert tr.device_status() == 0
     assert np.array_equal(sig0, sig1)
     assert torch.equal(out0[10], out1[10])
+
+
+def test_ploc_coincident_gaussians_build_a_balanced_tree(cuda_device):
+    """Coincident Gaussians give equal union areas for every pair of them. The PLOC tie-break pairs
+    equal boxes up all at once ((0,1), (2,3), ... in the list), so 30,000 copies of one Gaussian
+    build in a few iterations into a balanced tree, not a chain of one merge per iteration (which
+    would also overflow the traversal stack). The tree is walked and a trace runs without a loop
+    bound or stack overflow."""
+    import time
+
+    s = small_scene(n=30000, w=16, h=16, spp=1, max_bounces=2)
+    for k in ("build_pos", "build_rot", "build_scl", "build_dns", "density", "material", "sph", "shading_normal"):
+        s[k][1:] = s[k][0]  # every Gaussian a copy of the first
+    S = to_torch(s)
+    warm = make_tracer(bvh_builder="ploc")
+    warm.build_bvh(S["build_pos"][:64], S["build_rot"][:64], S["build_scl"][:64], S["build_dns"][:64], True, True)
+    torch.cuda.synchronize()
+    tr = make_tracer(bvh_builder="ploc")
+    t0 = time.perf_counter()
+    tr.build_bvh(S["build_pos"], S["build_rot"], S["build_scl"], S["build_dns"], True, True)
+    torch.cuda.synchronize()
+    seconds = time.perf_counter() - t0
+    assert seconds < 3.0, seconds
+    nodes, leaves = (t.numpy() for t in tr.debug_accel())
+    _, topo = _walk(nodes, leaves)
+    depth, stack = 0, [(0, 1)]
+    while stack:
+        i, dep = stack.pop()
+        depth = max(depth, dep)
+        stack += [(c, dep + 1) for c in topo[i] if c >= 0]
+    assert depth <= 40, depth  # log2(30000) ~ 15
+    _trace(tr, S, build=False, rebuild=False)
+    torch.cuda.synchronize()
+    assert tr.device_status() == 0
