@@ -158,6 +158,10 @@ class OptixTracer:
             raise ValueError(f"backward pipeline '{backward_pipeline}' is not available (only 'referenceBwd')")
         if primitive not in ("instances",):
             raise ValueError(f"primitive type '{primitive}' is not available (only 'instances')")
+        if storage not in N.STORAGES:
+            raise ValueError(f"storage '{storage}' is not one of {sorted(N.STORAGES)}")
+        if bvh_builder not in N.BVH_BUILDERS:
+            raise ValueError(f"bvh_builder '{bvh_builder}' is not one of {sorted(N.BVH_BUILDERS)}")
         self._lib = N.load()
         self.sph_degree = int(particle_radiance_sph_degree)
         self.enable_normals = bool(enable_normals)

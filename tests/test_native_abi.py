@@ -31,3 +31,17 @@ def test_abi_version_without_gpu():
 
 def test_built_for_sm100a():
     assert "arch=compute_100a,code=sm_100a" in " ".join(build.ARCH_FLAGS)
+
+
+def test_unknown_names_are_rejected_before_the_device():
+    """A misspelt storage or hierarchy builder fails with a clear ValueError before any device
+    call (CPU only)."""
+    import pytest
+
+    from ptir_b200 import OptixTracer
+
+    args = ("", "", "reference", "referenceBwd", "instances", 4, 0.0113, True, 3, True, True, True, False, False)
+    with pytest.raises(ValueError, match="bvh_builder"):
+        OptixTracer(*args, bvh_builder="sah")
+    with pytest.raises(ValueError, match="storage"):
+        OptixTracer(*args, storage="fp8")
